@@ -1,0 +1,194 @@
+/*
+ * physgpu.h -- C ABI of the B200 gravity library (libphysgpu.so).
+ *
+ * This is the drop-in boundary for the gravity path of Doritozzzz/phys-rs.
+ * The reference has no FFI for this path: its "plugin API" is a set of
+ * bevy_ecs system functions registered in a Schedule (src/main.rs:103-140).
+ * Each entry point below names the reference system or code whose work it
+ * replaces, so a Rust `extern "C"` block can wrap them
+ * in systems of the same signatures.
+ *
+ * Conventions
+ *  - Plain pointers and sizes; arrays are structure-of-arrays, f64, length n,
+ *    in the caller's (ECS query) order.  Host pointers unless the name says
+ *    "_device".
+ *  - Every call returns a status (PHYS_OK == 0).  No call aborts, throws or
+ *    traps; on error phys_last_error() describes it.
+ *  - A context owns one CUDA stream and all device memory it uses.  It is not
+ *    thread-safe (use one context per thread).  Calls are synchronous at
+ *    return, like the reference's blocking readback (src/gpu/buffers.rs:163-213),
+ *    except phys_verlet_steps_async.
+ *  - Body state stays resident on the device between calls, so multi-step
+ *    runs do not cross PCIe.
+ */
+#ifndef PHYSGPU_H
+#define PHYSGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PHYS_OK 0
+#define PHYS_ERR_ARG 1        /* bad argument (null pointer, size, enum)      */
+#define PHYS_ERR_CUDA 2       /* CUDA runtime error                           */
+#define PHYS_ERR_OOM 3        /* device or pinned allocation failed           */
+#define PHYS_ERR_NONFINITE 4  /* NaN/Inf in inputs or results                 */
+#define PHYS_ERR_TIMEOUT 5    /* a bounded device-side wait gave up           */
+#define PHYS_ERR_STATE 6      /* call order (e.g. no state uploaded)          */
+
+/* ---- force method / precision ----------------------------------------- */
+#define PHYS_DIRECT 0         /* brute_force_gravity_system (gravity.rs:27-74)         */
+#define PHYS_BARNES_HUT 1     /* barnes_hut_gravity_system (gravity_tree.rs:260-338)   */
+
+#define PHYS_F64_EXACT 0      /* reference op order, IEEE sqrt/div, no FMA, reference
+                                 summation order (direct: j order; BH: nested child
+                                 sums, insertion-order centre of mass): bit-identical
+                                 to the reference's f64 arithmetic                    */
+#define PHYS_F64 1            /* f64 with FMA and rsqrt, flat sums, parallel COM     */
+#define PHYS_F32C 2           /* f32 pair terms on double-float relative coordinates,
+                                 two-sum compensated f32 accumulation, f64 state     */
+
+typedef struct phys_ctx phys_ctx;
+
+/* UniverseConfig (src/core/config.rs:26-59) fields the gravity path reads,
+ * plus the method switches. */
+typedef struct phys_params {
+  double G;           /* gravitational_constant                               */
+  double eps;         /* softening_epsilon (eps^2 is added to r^2)            */
+  double theta;       /* barnes_hut_theta                                     */
+  int32_t method;     /* PHYS_DIRECT or PHYS_BARNES_HUT                       */
+  int32_t precision;  /* PHYS_F64_EXACT, PHYS_F64 or PHYS_F32C                */
+  int32_t leaf_cap;   /* BH leaf capacity: 1 = the reference octree; 2..16 =
+                         bucket leaves (criterion on the cell, exact pairs when
+                         opened).  F64_EXACT requires 1.                      */
+  int32_t flags;      /* reserved, must be 0                                  */
+} phys_params;
+
+/* Per-call device timings of the last force evaluation / step (CUDA events
+ * on the context's stream) and counters. */
+typedef struct phys_timings {
+  double total_ms;      /* whole last call                                    */
+  double bbox_ms;       /* bounding cube (gravity_tree.rs:305-317)            */
+  double keys_ms;       /* descent keys                                       */
+  double sort_ms;       /* radix sort + equal-prefix fixup                    */
+  double tree_ms;       /* topology, mass and centre of mass                  */
+  double walk_ms;       /* theta walk or direct-sum kernel                    */
+  double verlet_ms;     /* kick/drift kernels                                 */
+  uint64_t interactions;/* pair + monopole interactions of the last evaluation */
+  uint64_t launches;    /* kernels launched by this context since creation    */
+  int64_t nodes;        /* octree nodes of the last BH evaluation             */
+  int32_t max_depth;    /* guard depth D* of the last BH tree                 */
+  int32_t reserved;
+} phys_timings;
+
+/* ---- context ------------------------------------------------------------ */
+const char* phys_status_string(int status);
+const char* phys_last_error(const phys_ctx* ctx);
+int phys_ctx_create(int device, phys_ctx** out);
+int phys_ctx_destroy(phys_ctx* ctx);
+/* The cudaStream_t the context launches on (for callers that time or order
+ * work around it). */
+void* phys_ctx_stream(phys_ctx* ctx);
+int phys_last_timings(const phys_ctx* ctx, phys_timings* out);
+
+/* ---- body state --------------------------------------------------------- */
+/* Upload absolute positions, velocities (may be NULL: zero) and masses
+ * (the Mass / LocalPosition / Velocity components of the query).  Invalidates
+ * the cached acceleration. */
+int phys_state_upload(phys_ctx* ctx, int64_t n, const double* x, const double* y,
+                      const double* z, const double* vx, const double* vy, const double* vz,
+                      const double* m);
+/* Same, from (Sector, LocalPosition) pairs: positions are flattened on the
+ * device as (sector - origin) * sector_size + local with origin = the first
+ * body's sector (gravity.rs:38-47).  With bh_quirk != 0 every body is
+ * measured from its own sector, as barnes_hut_gravity_system does
+ * (gravity_tree.rs:280-291: `first` is never cleared). */
+int phys_state_upload_sectors(phys_ctx* ctx, int64_t n, const int64_t* sx, const int64_t* sy,
+                              const int64_t* sz, const double* lx, const double* ly,
+                              const double* lz, double sector_size, int32_t bh_quirk,
+                              const double* vx, const double* vy, const double* vz,
+                              const double* m);
+/* Set the Acceleration component (the a(x_n) a Velocity-Verlet tick starts
+ * from) and mark it valid for phys_verlet_steps. */
+int phys_state_set_accel(phys_ctx* ctx, const double* ax, const double* ay, const double* az);
+/* Download any of positions, velocities, accelerations (NULL skips). */
+int phys_state_download(phys_ctx* ctx, double* x, double* y, double* z, double* vx, double* vy,
+                        double* vz, double* ax, double* ay, double* az);
+int64_t phys_state_size(const phys_ctx* ctx);
+
+/* Per-component access to the device-resident state, one ECS component at a
+ * time (src/components/dynamics.rs:13-37, src/core/coordinates.rs:26).
+ * MASS uses only the first pointer.  Writing POSITION or MASS invalidates the
+ * cached acceleration; writing ACCELERATION marks it valid. */
+#define PHYS_COMP_POSITION 0
+#define PHYS_COMP_VELOCITY 1
+#define PHYS_COMP_ACCELERATION 2
+#define PHYS_COMP_PREV_ACCELERATION 3
+#define PHYS_COMP_MASS 4
+int phys_component_write(phys_ctx* ctx, int32_t component, const double* a, const double* b,
+                         const double* c);
+int phys_component_read(phys_ctx* ctx, int32_t component, double* a, double* b, double* c);
+
+/* ---- gravity (one force evaluation at the uploaded positions) ---------- */
+/* brute_force_gravity_system / barnes_hut_gravity_system: ADDS the
+ * gravitational force to fx/fy/fz (Force += F, gravity.rs:71-73,
+ * gravity_tree.rs:333-337).  Returns without touching them for n < 2
+ * (gravity.rs:49-51). */
+int phys_gravity_forces(phys_ctx* ctx, const phys_params* p, double* fx, double* fy, double* fz);
+/* The same evaluation followed by compute_acceleration_system (a = F/m,
+ * integrators.rs:110-118) with Force reset to zero first (forces.rs:15-19).
+ * Writes ax/ay/az (each may be NULL to keep the result on the device only)
+ * and caches a(x) for phys_verlet_steps. */
+int phys_gravity_accel(phys_ctx* ctx, const phys_params* p, double* ax, double* ay, double* az);
+
+/* ---- integration -------------------------------------------------------- */
+/* nsteps Velocity-Verlet ticks on the device-resident state: each tick is
+ * velocity_verlet_position_system (integrators.rs:63-83), a force evaluation
+ * + a = F/m, velocity_verlet_velocity_system (integrators.rs:92-104).
+ * The reference evaluates gravity twice per tick (src/main.rs:109,128); the
+ * first evaluation repeats the previous tick's second one at the same
+ * positions, so it is taken from the cache: the trajectory is the same. */
+int phys_verlet_steps(phys_ctx* ctx, const phys_params* p, double dt, int64_t nsteps);
+/* The two halves of the tick as separate systems, on the device state:
+ * velocity_verlet_position_system (PreviousAcceleration = Acceleration;
+ * x += v dt + a dt^2/2) and velocity_verlet_velocity_system
+ * (v += (PreviousAcceleration + Acceleration) dt/2). */
+int phys_vv_position_step(phys_ctx* ctx, double dt);
+int phys_vv_velocity_step(phys_ctx* ctx, double dt);
+/* As phys_verlet_steps but returns once the work is enqueued on the
+ * context's stream (host sync only for the BH node count). */
+int phys_verlet_steps_async(phys_ctx* ctx, const phys_params* p, double dt, int64_t nsteps);
+
+/* ---- diagnostics (src/physics/energy.rs:21-56, integrators.rs:123-129) -- */
+/* out[0] = kinetic energy sum 1/2 m v^2, out[1] = unsoftened potential energy
+ * -sum_{i<j} G m_i m_j / r (r^2 == 0 pairs skipped), out[2..4] = total linear
+ * momentum sum m v.  f64 on the device with compensated sums. */
+int phys_diagnostics(phys_ctx* ctx, double G, double* out5);
+
+/* ---- Barnes-Hut tree export (parity checks) ----------------------------- */
+/* Builds the octree for the uploaded positions with params p (method is
+ * ignored) and exports, in pre-order over non-empty cells (children in
+ * octant order 0..7, the order compute_force visits them):
+ *   depth, count (bodies in the cell), mass, com (3*cap, xyz interleaved),
+ *   leaf_body (stored body of a leaf, -1 for internal cells),
+ *   body_leaf (per body: id of the leaf whose cell holds it),
+ * plus per body the 120-bit descent key (keys_hi: octants 0..20, keys_lo:
+ * octants 21..39), the sorted permutation, and root4 = (cx, cy, cz, half).
+ * Any output pointer may be NULL.  *nnodes receives the node count; arrays
+ * are filled up to cap entries. */
+int phys_bh_export(phys_ctx* ctx, const phys_params* p, int64_t cap, int64_t* nnodes,
+                   int32_t* depth, int64_t* count, double* mass, double* com,
+                   int64_t* leaf_body, int64_t* body_leaf, uint64_t* keys_hi,
+                   uint64_t* keys_lo, int64_t* perm, double* root4);
+
+/* ---- measured pipe peaks (roofline denominators) ----------------------- */
+/* Times FFMA / DFMA loops on every SM; returns TFLOP/s counting an FMA as 2. */
+int phys_probe_peaks(phys_ctx* ctx, double* fp32_tflops, double* fp64_tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PHYSGPU_H */

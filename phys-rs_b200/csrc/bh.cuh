@@ -1,0 +1,52 @@
+// Barnes-Hut tree layout shared by the build (tree.cu) and the walk (walk.cu).
+//
+// Nodes are the non-empty cells of the octree in pre-order (children in
+// octant order 0..7, the order OctreeNode::compute_force visits them,
+// gravity_tree.rs:200-204).  Per node:
+//   link  int4  {next, start, end, meta}
+//         next  = pre-order index after the node's subtree (skip pointer)
+//         start, end = the cell's bodies in key-sorted order [start, end)
+//         meta  = depth | kLeaf | kGuard | kGate
+//   rec   walk record: for a one-body leaf (and a guard leaf with leaf_cap 1)
+//         the stored body's own position and mass; otherwise the cell's
+//         centre of mass and total mass.  double4 for f64 walks; for f32
+//         walks two float4: (x_hi, y_hi, z_hi, m) and (x_lo, y_lo, z_lo, 0).
+//   mc    double4 aggregate (com x, y, z, total mass) of all bodies in the
+//         cell (the reference's center_of_mass / total_mass fields).
+#pragma once
+
+#include "common.cuh"
+
+namespace phys {
+
+constexpr int kMetaDepth = 0xff;
+constexpr int kMetaLeaf = 1 << 8;    // leaf cell (no children in this tree)
+constexpr int kMetaGuard = 1 << 9;   // leaf at the guard depth D* (gravity_tree.rs:121-126)
+constexpr int kMetaGate = 1 << 10;   // total_mass > 0 (children are visited only then,
+                                     // gravity_tree.rs:201)
+
+struct BhTree {
+  int64_t n = 0;
+  int64_t nnodes = 0;
+  int leaf_cap = 1;
+  const int4* link = nullptr;
+  const double4* rec64 = nullptr;
+  const float4* rec_hi = nullptr;
+  const float4* rec_lo = nullptr;
+  const double4* mc = nullptr;
+  const uint32_t* perm = nullptr;     // sorted position -> caller index
+  const double4* body64 = nullptr;    // sorted bodies (x, y, z, m)
+  const float4* body_hi = nullptr;    // sorted bodies, double-float hi + f32 mass
+  const float4* body_lo = nullptr;
+  const TreeHeader* hdr = nullptr;
+  const uint64_t* keys_hi_sorted = nullptr;  // descent keys, octants 0..20, sorted
+  const uint64_t* keys_lo = nullptr;         // octants 21..39, caller order
+};
+
+// tree.cu
+int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t);
+// walk.cu
+int bh_walk(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force, double* ox,
+            double* oy, double* oz);
+
+}  // namespace phys

@@ -1,0 +1,183 @@
+// Internal declarations shared by the libphysgpu translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "../../include/physgpu.h"
+
+namespace phys {
+
+constexpr int kMaxDepth = 40;            // gravity_tree.rs:30
+constexpr double kMinNodeSize = 1e-8;    // gravity_tree.rs:34
+constexpr int kMaxLevels = kMaxDepth + 1;
+constexpr int kMaxLeafCap = 16;
+
+// Device status word bits (reduced into ctx->d_status by kernels).
+constexpr int kStatNonfinite = 1;
+constexpr int kStatTimeout = 2;
+constexpr int kStatOverflow = 4;
+
+// Growable device buffer (bytes).  Memory is released by the context.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+// Per-tree constants written on the device by the bbox kernel and read by
+// every later kernel of the force evaluation (no host round trip).
+struct TreeHeader {
+  double center[3];
+  double half;                   // root half size (gravity_tree.rs:316)
+  double theta2;                 // theta * theta
+  double s2[kMaxLevels];         // (2 h_d)^2 per depth, h_d = half * 0.5^d by repeated halving
+  int32_t dstar;                 // guard depth: first d with d >= 40 or h_d < 1e-8
+  int32_t nonfinite;             // any non-finite input coordinate
+  int64_t nnodes;                // nodes of the current tree
+};
+
+}  // namespace phys
+
+struct phys_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  uint64_t launches = 0;
+  phys_timings tm{};
+
+  // ---- body state (SoA, caller order) ----
+  int64_t n = 0, cap = 0;
+  double *x = nullptr, *y = nullptr, *z = nullptr;
+  double *vx = nullptr, *vy = nullptr, *vz = nullptr;
+  double *m = nullptr;
+  double *ax = nullptr, *ay = nullptr, *az = nullptr;     // Acceleration
+  double *pax = nullptr, *pay = nullptr, *paz = nullptr;  // PreviousAcceleration
+  double *fx = nullptr, *fy = nullptr, *fz = nullptr;     // gravity force scratch
+  bool accel_valid = false;
+  phys_params accel_params{};
+  bool last_eval_bh = false;   // the interaction count lives in d_counter
+
+  // ---- small device scalars ----
+  int32_t* d_status = nullptr;               // kStat* bits
+  unsigned long long* d_counter = nullptr;   // interaction counter
+  phys::TreeHeader* d_hdr = nullptr;
+  double* d_partials = nullptr;              // reduction partials (diagnostics, bbox)
+  size_t partials_cap = 0;
+
+  // ---- host staging (pinned) ----
+  void* h_stage = nullptr;
+  size_t h_stage_bytes = 0;
+  int32_t* h_small = nullptr;                // pinned scalars for status / counts
+
+  // ---- workspace buffers (grown on demand, named) ----
+  phys::DevBuf ws[48];
+
+  // ---- events for per-phase timings ----
+  cudaEvent_t ev[12] = {};
+};
+
+// ---- helpers (ctx.cu) ----
+namespace phys {
+int fail(phys_ctx* c, int code, const char* fmt, ...);
+int cuda_fail(phys_ctx* c, cudaError_t e, const char* what);
+// Ensure workspace slot `slot` holds at least `bytes`; returns device pointer.
+void* ws_get(phys_ctx* c, int slot, size_t bytes, int* status);
+int ensure_pinned(phys_ctx* c, size_t bytes);
+int check_launch(phys_ctx* c, const char* what);
+int read_status(phys_ctx* c, int32_t* out);
+
+// Workspace slot ids.
+enum WsSlot {
+  WS_KEYS_HI = 0, WS_KEYS_LO, WS_IDX, WS_KEYS_HI_ALT, WS_IDX_ALT, WS_HIST,
+  WS_LCP, WS_NCOUNT, WS_NFIRST, WS_SCAN_TMP,
+  WS_LINK, WS_NODE_PM, WS_NODE_HI, WS_NODE_LO, WS_PARENT, WS_ARRIVE, WS_NODE_S,
+  WS_BODY_PM, WS_BODY_HI, WS_BODY_LO,
+  WS_KEEP, WS_NEWID, WS_LINK2,
+  WS_ENTRIES, WS_ENTRIES_ALT, WS_EOFF,
+  WS_DIRECT_PART, WS_ADJ0, WS_ADJ1, WS_ADJ2, WS_ADJ3, WS_ADJ4,
+  WS_ENS0, WS_ENS1, WS_ENS2, WS_ENS3, WS_ENS4, WS_ENS5, WS_ENS6, WS_ENS7,
+  WS_COUNT_
+};
+
+// ---- kernels' host launchers (per .cu file) ----
+// direct.cu
+int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, double* oy,
+                double* oz);
+// tree.cu
+int bh_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, double* oy,
+            double* oz);
+int bh_export(phys_ctx* c, const phys_params* p, int64_t cap, int64_t* nnodes, int32_t* depth,
+              int64_t* count, double* mass, double* com, int64_t* leaf_body, int64_t* body_leaf,
+              uint64_t* keys_hi, uint64_t* keys_lo, int64_t* perm, double* root4);
+// sort.cu
+int radix_sort_u64(phys_ctx* c, uint64_t* keys, uint32_t* vals, uint64_t* keys_alt,
+                   uint32_t* vals_alt, int64_t n, int begin_bit, int end_bit, bool* result_in_alt);
+int scan_exclusive_i32(phys_ctx* c, const int32_t* in, int32_t* out, int64_t n);
+// verlet.cu
+int verlet_drift(phys_ctx* c, double dt);
+int verlet_kick(phys_ctx* c, double dt);
+int verlet_kick_drift(phys_ctx* c, double dt);
+int flatten_sectors(phys_ctx* c, const int64_t* dsx, const int64_t* dsy, const int64_t* dsz,
+                    const double* dlx, const double* dly, const double* dlz, double sector_size,
+                    int bh_quirk);
+// diag.cu
+int diagnostics(phys_ctx* c, double G, double* out5);
+int probe_peaks(phys_ctx* c, double* fp32, double* fp64);
+}  // namespace phys
+
+#define PHYS_LAUNCH(c, kernel, grid, block, smem, ...)                     \
+  do {                                                                     \
+    kernel<<<(grid), (block), (smem), (c)->stream>>>(__VA_ARGS__);          \
+    (c)->launches++;                                                       \
+    int _st = phys::check_launch((c), #kernel);                            \
+    if (_st) return _st;                                                   \
+  } while (0)
+
+#define PHYS_CUDA(c, call)                                                 \
+  do {                                                                     \
+    cudaError_t _e = (call);                                               \
+    if (_e != cudaSuccess) return phys::cuda_fail((c), _e, #call);         \
+  } while (0)
+
+#define PHYS_TRY(expr)            \
+  do {                            \
+    int _s = (expr);              \
+    if (_s) return _s;            \
+  } while (0)
+
+// ---- device helpers ----
+namespace phys {
+
+// IEEE double ops that the compiler may not contract into FMAs: the
+// reference's Rust arithmetic rounds every + and * separately.
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double xsqrt(double a) { return __dsqrt_rn(a); }
+// glam DVec3::length_squared: (x*x + y*y) + z*z
+__device__ __forceinline__ double xlen2(double x, double y, double z) {
+  return xadd(xadd(xmul(x, x), xmul(y, y)), xmul(z, z));
+}
+
+// Knuth two-sum: s + e == a + b exactly.
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+  s = __fadd_rn(a, b);
+  float bb = __fsub_rn(s, a);
+  e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+
+// Split a double into a float pair with hi + lo ~= v to ~2^-48 relative.
+__device__ __forceinline__ void split_df(double v, float& hi, float& lo) {
+  hi = __double2float_rn(v);
+  lo = __double2float_rn(v - (double)hi);
+}
+
+__host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+__host__ __device__ inline int64_t min64(int64_t a, int64_t b) { return a < b ? a : b; }
+
+}  // namespace phys

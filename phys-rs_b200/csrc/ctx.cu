@@ -1,0 +1,567 @@
+// Context, device state, error handling and the public entry points that
+// orchestrate the kernels of the other translation units.
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+
+namespace phys {
+
+int fail(phys_ctx* c, int code, const char* fmt, ...) {
+  if (c) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    c->err = buf;
+  }
+  return code;
+}
+
+int cuda_fail(phys_ctx* c, cudaError_t e, const char* what) {
+  int code = (e == cudaErrorMemoryAllocation) ? PHYS_ERR_OOM : PHYS_ERR_CUDA;
+  cudaGetLastError();  // clear non-sticky errors
+  return fail(c, code, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+int check_launch(phys_ctx* c, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(c, e, what);
+  return PHYS_OK;
+}
+
+void* ws_get(phys_ctx* c, int slot, size_t bytes, int* status) {
+  DevBuf& b = c->ws[slot];
+  if (bytes == 0) bytes = 16;
+  if (b.bytes >= bytes) return b.p;
+  if (b.p) {
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+      *status = cuda_fail(c, e, "cudaStreamSynchronize(ws grow)");
+      return nullptr;
+    }
+    cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+  }
+  size_t want = bytes + bytes / 8;  // headroom for slowly growing sizes
+  want = (want + 255) & ~size_t(255);
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e != cudaSuccess) {
+    b.p = nullptr;
+    *status = cuda_fail(c, e, "cudaMalloc(workspace)");
+    return nullptr;
+  }
+  b.bytes = want;
+  return b.p;
+}
+
+int ensure_pinned(phys_ctx* c, size_t bytes) {
+  if (c->h_stage_bytes >= bytes) return PHYS_OK;
+  if (c->h_stage) {
+    cudaStreamSynchronize(c->stream);
+    cudaFreeHost(c->h_stage);
+    c->h_stage = nullptr;
+    c->h_stage_bytes = 0;
+  }
+  cudaError_t e = cudaMallocHost(&c->h_stage, bytes);
+  if (e != cudaSuccess) {
+    c->h_stage = nullptr;
+    return cuda_fail(c, e, "cudaMallocHost(staging)");
+  }
+  c->h_stage_bytes = bytes;
+  return PHYS_OK;
+}
+
+int read_status(phys_ctx* c, int32_t* out) {
+  PHYS_CUDA(c, cudaMemcpyAsync(c->h_small, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                               c->stream));
+  PHYS_CUDA(c, cudaMemcpyAsync(c->h_small + 2, c->d_counter, sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, c->stream));
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  *out = c->h_small[0];
+  if (c->last_eval_bh) {
+    unsigned long long v;
+    memcpy(&v, c->h_small + 2, sizeof v);
+    c->tm.interactions = v;
+  }
+  return PHYS_OK;
+}
+
+}  // namespace phys
+
+using namespace phys;
+
+namespace {
+
+int ensure_state(phys_ctx* c, int64_t n) {
+  if (n <= c->cap) return PHYS_OK;
+  if (c->x) {
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->x);
+    c->x = nullptr;
+    c->cap = 0;
+  }
+  int64_t cap = n < 1024 ? 1024 : n;
+  double* base = nullptr;
+  cudaError_t e = cudaMalloc(&base, sizeof(double) * 16 * size_t(cap));
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc(state)");
+  double** slots[16] = {&c->x,  &c->y,  &c->z,  &c->vx,  &c->vy,  &c->vz,  &c->m,  &c->ax,
+                        &c->ay, &c->az, &c->pax, &c->pay, &c->paz, &c->fx, &c->fy, &c->fz};
+  for (int k = 0; k < 16; ++k) *slots[k] = base + size_t(k) * cap;
+  c->cap = cap;
+  return PHYS_OK;
+}
+
+int h2d(phys_ctx* c, double* dst, const double* src, int64_t n) {
+  if (src) {
+    PHYS_CUDA(c, cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  } else {
+    PHYS_CUDA(c, cudaMemsetAsync(dst, 0, sizeof(double) * n, c->stream));
+  }
+  return PHYS_OK;
+}
+
+int d2h(phys_ctx* c, double* dst, const double* src, int64_t n) {
+  if (dst)
+    PHYS_CUDA(c, cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  return PHYS_OK;
+}
+
+int check_params(phys_ctx* c, const phys_params* p) {
+  if (!p) return fail(c, PHYS_ERR_ARG, "params is NULL");
+  if (p->method != PHYS_DIRECT && p->method != PHYS_BARNES_HUT)
+    return fail(c, PHYS_ERR_ARG, "unknown method %d", p->method);
+  if (p->precision < PHYS_F64_EXACT || p->precision > PHYS_F32C)
+    return fail(c, PHYS_ERR_ARG, "unknown precision %d", p->precision);
+  if (p->leaf_cap < 1 || p->leaf_cap > kMaxLeafCap)
+    return fail(c, PHYS_ERR_ARG, "leaf_cap %d outside 1..%d", p->leaf_cap, kMaxLeafCap);
+  if (p->method == PHYS_BARNES_HUT && p->precision == PHYS_F64_EXACT && p->leaf_cap != 1)
+    return fail(c, PHYS_ERR_ARG, "F64_EXACT Barnes-Hut follows the reference octree: leaf_cap 1");
+  if (p->flags != 0) return fail(c, PHYS_ERR_ARG, "flags must be 0");
+  if (!(p->theta >= 0.0)) return fail(c, PHYS_ERR_ARG, "theta must be >= 0");
+  return PHYS_OK;
+}
+
+bool same_params(const phys_params& a, const phys_params& b) {
+  return a.G == b.G && a.eps == b.eps && a.theta == b.theta && a.method == b.method &&
+         a.precision == b.precision && a.leaf_cap == b.leaf_cap;
+}
+
+// One force evaluation on the device: accelerations into c->ax.. (want_force
+// false) or forces into c->fx.. (want_force true).
+int eval(phys_ctx* c, const phys_params* p, bool want_force) {
+  double* ox = want_force ? c->fx : c->ax;
+  double* oy = want_force ? c->fy : c->ay;
+  double* oz = want_force ? c->fz : c->az;
+  if (c->n < 2) {  // gravity.rs:49-51: no pairs, forces stay zero
+    PHYS_CUDA(c, cudaMemsetAsync(ox, 0, sizeof(double) * c->n, c->stream));
+    PHYS_CUDA(c, cudaMemsetAsync(oy, 0, sizeof(double) * c->n, c->stream));
+    PHYS_CUDA(c, cudaMemsetAsync(oz, 0, sizeof(double) * c->n, c->stream));
+    c->tm.interactions = 0;
+    return PHYS_OK;
+  }
+  c->last_eval_bh = p->method == PHYS_BARNES_HUT;
+  if (p->method == PHYS_DIRECT) return direct_eval(c, p, want_force, ox, oy, oz);
+  return bh_eval(c, p, want_force, ox, oy, oz);
+}
+
+float ev_ms(cudaEvent_t a, cudaEvent_t b);
+
+int finish_status(phys_ctx* c) {
+  int32_t st = 0;
+  PHYS_TRY(read_status(c, &st));
+  if (c->last_eval_bh) {
+    c->tm.bbox_ms = ev_ms(c->ev[2], c->ev[3]);
+    c->tm.keys_ms = ev_ms(c->ev[3], c->ev[4]);
+    c->tm.sort_ms = ev_ms(c->ev[4], c->ev[5]);
+    c->tm.tree_ms = ev_ms(c->ev[5], c->ev[6]);
+  }
+  c->tm.walk_ms = ev_ms(c->ev[6], c->ev[7]);
+  if (st & kStatTimeout) return fail(c, PHYS_ERR_TIMEOUT, "a bounded device wait timed out");
+  if (st & kStatOverflow) return fail(c, PHYS_ERR_CUDA, "device workspace overflow");
+  if (st & kStatNonfinite)
+    return fail(c, PHYS_ERR_NONFINITE, "non-finite value in positions, masses or results");
+  return PHYS_OK;
+}
+
+int reset_status(phys_ctx* c) {
+  PHYS_CUDA(c, cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream));
+  return PHYS_OK;
+}
+
+float ev_ms(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+    cudaGetLastError();
+    return 0.f;
+  }
+  return ms;
+}
+
+int verlet_steps(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, bool sync) {
+  PHYS_TRY(check_params(c, p));
+  if (nsteps < 0) return fail(c, PHYS_ERR_ARG, "nsteps < 0");
+  if (c->n == 0) return fail(c, PHYS_ERR_STATE, "no body state uploaded");
+  if (!(dt == dt)) return fail(c, PHYS_ERR_ARG, "dt is NaN");
+  PHYS_TRY(reset_status(c));
+  PHYS_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+  if (!c->accel_valid || !same_params(c->accel_params, *p)) {
+    PHYS_TRY(eval(c, p, false));  // chain 1 force pass of the first tick
+    c->accel_valid = true;
+    c->accel_params = *p;
+  }
+  for (int64_t s = 0; s < nsteps; ++s) {
+    if (s == 0) PHYS_TRY(verlet_drift(c, dt));
+    c->accel_valid = false;
+    PHYS_TRY(eval(c, p, false));  // chain 2 force pass at x_{n+1}
+    c->accel_valid = true;
+    if (s + 1 < nsteps)
+      PHYS_TRY(verlet_kick_drift(c, dt));  // velocity step of tick s, position step of s+1
+    else
+      PHYS_TRY(verlet_kick(c, dt));
+  }
+  PHYS_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+  if (sync) {
+    PHYS_TRY(finish_status(c));
+    c->tm.total_ms = ev_ms(c->ev[0], c->ev[1]);
+  }
+  return PHYS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* phys_status_string(int s) {
+  switch (s) {
+    case PHYS_OK: return "ok";
+    case PHYS_ERR_ARG: return "invalid argument";
+    case PHYS_ERR_CUDA: return "CUDA error";
+    case PHYS_ERR_OOM: return "out of memory";
+    case PHYS_ERR_NONFINITE: return "non-finite value";
+    case PHYS_ERR_TIMEOUT: return "device wait timed out";
+    case PHYS_ERR_STATE: return "invalid call order";
+    default: return "unknown status";
+  }
+}
+
+const char* phys_last_error(const phys_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int phys_ctx_create(int device, phys_ctx** out) {
+  if (!out) return PHYS_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return PHYS_ERR_CUDA;
+  }
+  if (device < 0 || device >= ndev) return PHYS_ERR_ARG;
+  phys_ctx* c = new (std::nothrow) phys_ctx();
+  if (!c) return PHYS_ERR_OOM;
+  c->device = device;
+  int st = PHYS_OK;
+  do {
+    if ((e = cudaSetDevice(device)) != cudaSuccess) { st = cuda_fail(c, e, "cudaSetDevice"); break; }
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+      st = cuda_fail(c, e, "cudaStreamCreate");
+      break;
+    }
+    for (auto& ev : c->ev)
+      if ((e = cudaEventCreate(&ev)) != cudaSuccess) { st = cuda_fail(c, e, "cudaEventCreate"); break; }
+    if (st) break;
+    char* small = nullptr;
+    if ((e = cudaMalloc(&small, 4096)) != cudaSuccess) { st = cuda_fail(c, e, "cudaMalloc(small)"); break; }
+    c->d_status = reinterpret_cast<int32_t*>(small);
+    c->d_counter = reinterpret_cast<unsigned long long*>(small + 256);
+    c->d_hdr = reinterpret_cast<TreeHeader*>(small + 512);
+    if ((e = cudaMemset(small, 0, 4096)) != cudaSuccess) { st = cuda_fail(c, e, "cudaMemset"); break; }
+    if ((e = cudaMallocHost(&c->h_small, 4096)) != cudaSuccess) {
+      st = cuda_fail(c, e, "cudaMallocHost(small)");
+      break;
+    }
+  } while (0);
+  if (st) {
+    phys_ctx_destroy(c);
+    return st;
+  }
+  *out = c;
+  return PHYS_OK;
+}
+
+int phys_ctx_destroy(phys_ctx* c) {
+  if (!c) return PHYS_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto& b : c->ws)
+    if (b.p) cudaFree(b.p);
+  if (c->x) cudaFree(c->x);
+  if (c->d_status) cudaFree(c->d_status);
+  if (c->d_partials) cudaFree(c->d_partials);
+  if (c->h_stage) cudaFreeHost(c->h_stage);
+  if (c->h_small) cudaFreeHost(c->h_small);
+  for (auto& ev : c->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  cudaGetLastError();
+  delete c;
+  return PHYS_OK;
+}
+
+void* phys_ctx_stream(phys_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int phys_last_timings(const phys_ctx* c, phys_timings* out) {
+  if (!c || !out) return PHYS_ERR_ARG;
+  *out = c->tm;
+  out->launches = c->launches;
+  return PHYS_OK;
+}
+
+int64_t phys_state_size(const phys_ctx* c) { return c ? c->n : -1; }
+
+int phys_state_upload(phys_ctx* c, int64_t n, const double* x, const double* y, const double* z,
+                      const double* vx, const double* vy, const double* vz, const double* m) {
+  if (!c) return PHYS_ERR_ARG;
+  if (n < 0 || n > (int64_t(1) << 31) - 1) return fail(c, PHYS_ERR_ARG, "n=%lld out of range", (long long)n);
+  if (n > 0 && (!x || !y || !z || !m)) return fail(c, PHYS_ERR_ARG, "positions and masses are required");
+  PHYS_CUDA(c, cudaSetDevice(c->device));
+  PHYS_TRY(ensure_state(c, n));
+  c->n = n;
+  c->accel_valid = false;
+  if (n == 0) return PHYS_OK;
+  PHYS_TRY(h2d(c, c->x, x, n));
+  PHYS_TRY(h2d(c, c->y, y, n));
+  PHYS_TRY(h2d(c, c->z, z, n));
+  PHYS_TRY(h2d(c, c->vx, vx, n));
+  PHYS_TRY(h2d(c, c->vy, vy, n));
+  PHYS_TRY(h2d(c, c->vz, vz, n));
+  PHYS_TRY(h2d(c, c->m, m, n));
+  PHYS_TRY(h2d(c, c->ax, nullptr, n));
+  PHYS_TRY(h2d(c, c->ay, nullptr, n));
+  PHYS_TRY(h2d(c, c->az, nullptr, n));
+  PHYS_TRY(h2d(c, c->pax, nullptr, n));
+  PHYS_TRY(h2d(c, c->pay, nullptr, n));
+  PHYS_TRY(h2d(c, c->paz, nullptr, n));
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PHYS_OK;
+}
+
+int phys_state_upload_sectors(phys_ctx* c, int64_t n, const int64_t* sx, const int64_t* sy,
+                              const int64_t* sz, const double* lx, const double* ly,
+                              const double* lz, double sector_size, int32_t bh_quirk,
+                              const double* vx, const double* vy, const double* vz,
+                              const double* m) {
+  if (!c) return PHYS_ERR_ARG;
+  if (n < 0 || n > (int64_t(1) << 31) - 1) return fail(c, PHYS_ERR_ARG, "n out of range");
+  if (n > 0 && (!sx || !sy || !sz || !lx || !ly || !lz || !m))
+    return fail(c, PHYS_ERR_ARG, "sectors, local positions and masses are required");
+  PHYS_CUDA(c, cudaSetDevice(c->device));
+  PHYS_TRY(ensure_state(c, n));
+  c->n = n;
+  c->accel_valid = false;
+  if (n == 0) return PHYS_OK;
+  // Stage sectors in the force scratch arrays (same size as int64) and the
+  // local positions in x/y/z, then flatten in place on the device.
+  int64_t* dsx = reinterpret_cast<int64_t*>(c->fx);
+  int64_t* dsy = reinterpret_cast<int64_t*>(c->fy);
+  int64_t* dsz = reinterpret_cast<int64_t*>(c->fz);
+  PHYS_CUDA(c, cudaMemcpyAsync(dsx, sx, 8 * n, cudaMemcpyHostToDevice, c->stream));
+  PHYS_CUDA(c, cudaMemcpyAsync(dsy, sy, 8 * n, cudaMemcpyHostToDevice, c->stream));
+  PHYS_CUDA(c, cudaMemcpyAsync(dsz, sz, 8 * n, cudaMemcpyHostToDevice, c->stream));
+  PHYS_TRY(h2d(c, c->x, lx, n));
+  PHYS_TRY(h2d(c, c->y, ly, n));
+  PHYS_TRY(h2d(c, c->z, lz, n));
+  PHYS_TRY(flatten_sectors(c, dsx, dsy, dsz, c->x, c->y, c->z, sector_size, bh_quirk));
+  PHYS_TRY(h2d(c, c->vx, vx, n));
+  PHYS_TRY(h2d(c, c->vy, vy, n));
+  PHYS_TRY(h2d(c, c->vz, vz, n));
+  PHYS_TRY(h2d(c, c->m, m, n));
+  PHYS_TRY(h2d(c, c->ax, nullptr, n));
+  PHYS_TRY(h2d(c, c->ay, nullptr, n));
+  PHYS_TRY(h2d(c, c->az, nullptr, n));
+  PHYS_TRY(h2d(c, c->pax, nullptr, n));
+  PHYS_TRY(h2d(c, c->pay, nullptr, n));
+  PHYS_TRY(h2d(c, c->paz, nullptr, n));
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PHYS_OK;
+}
+
+int phys_state_set_accel(phys_ctx* c, const double* ax, const double* ay, const double* az) {
+  if (!c) return PHYS_ERR_ARG;
+  if (!ax || !ay || !az) return fail(c, PHYS_ERR_ARG, "accelerations are required");
+  PHYS_TRY(h2d(c, c->ax, ax, c->n));
+  PHYS_TRY(h2d(c, c->ay, ay, c->n));
+  PHYS_TRY(h2d(c, c->az, az, c->n));
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->accel_valid = true;
+  c->accel_params.method = -1;  // valid for any params: the caller vouches for it
+  return PHYS_OK;
+}
+
+int phys_state_download(phys_ctx* c, double* x, double* y, double* z, double* vx, double* vy,
+                        double* vz, double* ax, double* ay, double* az) {
+  if (!c) return PHYS_ERR_ARG;
+  int64_t n = c->n;
+  if (n == 0) return PHYS_OK;
+  PHYS_TRY(d2h(c, x, c->x, n));
+  PHYS_TRY(d2h(c, y, c->y, n));
+  PHYS_TRY(d2h(c, z, c->z, n));
+  PHYS_TRY(d2h(c, vx, c->vx, n));
+  PHYS_TRY(d2h(c, vy, c->vy, n));
+  PHYS_TRY(d2h(c, vz, c->vz, n));
+  PHYS_TRY(d2h(c, ax, c->ax, n));
+  PHYS_TRY(d2h(c, ay, c->ay, n));
+  PHYS_TRY(d2h(c, az, c->az, n));
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PHYS_OK;
+}
+
+static int comp_ptrs(phys_ctx* c, int32_t comp, double** a, double** b, double** d) {
+  switch (comp) {
+    case PHYS_COMP_POSITION: *a = c->x; *b = c->y; *d = c->z; return PHYS_OK;
+    case PHYS_COMP_VELOCITY: *a = c->vx; *b = c->vy; *d = c->vz; return PHYS_OK;
+    case PHYS_COMP_ACCELERATION: *a = c->ax; *b = c->ay; *d = c->az; return PHYS_OK;
+    case PHYS_COMP_PREV_ACCELERATION: *a = c->pax; *b = c->pay; *d = c->paz; return PHYS_OK;
+    case PHYS_COMP_MASS: *a = c->m; *b = nullptr; *d = nullptr; return PHYS_OK;
+    default: return fail(c, PHYS_ERR_ARG, "unknown component %d", comp);
+  }
+}
+
+int phys_component_write(phys_ctx* c, int32_t comp, const double* a, const double* b,
+                         const double* d) {
+  if (!c) return PHYS_ERR_ARG;
+  if (c->n == 0) return fail(c, PHYS_ERR_STATE, "no body state uploaded");
+  double *da, *db, *dd;
+  PHYS_TRY(comp_ptrs(c, comp, &da, &db, &dd));
+  if (!a || (db && (!b || !d))) return fail(c, PHYS_ERR_ARG, "component arrays are required");
+  PHYS_TRY(h2d(c, da, a, c->n));
+  if (db) {
+    PHYS_TRY(h2d(c, db, b, c->n));
+    PHYS_TRY(h2d(c, dd, d, c->n));
+  }
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (comp == PHYS_COMP_POSITION || comp == PHYS_COMP_MASS) c->accel_valid = false;
+  if (comp == PHYS_COMP_ACCELERATION) {
+    c->accel_valid = true;
+    c->accel_params.method = -1;
+  }
+  return PHYS_OK;
+}
+
+int phys_component_read(phys_ctx* c, int32_t comp, double* a, double* b, double* d) {
+  if (!c) return PHYS_ERR_ARG;
+  double *da, *db, *dd;
+  PHYS_TRY(comp_ptrs(c, comp, &da, &db, &dd));
+  if (c->n == 0) return PHYS_OK;
+  PHYS_TRY(d2h(c, a, da, c->n));
+  if (db) {
+    PHYS_TRY(d2h(c, b, db, c->n));
+    PHYS_TRY(d2h(c, d, dd, c->n));
+  }
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PHYS_OK;
+}
+
+int phys_vv_position_step(phys_ctx* c, double dt) {
+  if (!c) return PHYS_ERR_ARG;
+  if (c->n == 0) return fail(c, PHYS_ERR_STATE, "no body state uploaded");
+  PHYS_TRY(reset_status(c));
+  PHYS_TRY(verlet_drift(c, dt));
+  c->accel_valid = false;
+  return finish_status(c);
+}
+
+int phys_vv_velocity_step(phys_ctx* c, double dt) {
+  if (!c) return PHYS_ERR_ARG;
+  if (c->n == 0) return fail(c, PHYS_ERR_STATE, "no body state uploaded");
+  PHYS_TRY(reset_status(c));
+  PHYS_TRY(verlet_kick(c, dt));
+  return finish_status(c);
+}
+
+int phys_gravity_forces(phys_ctx* c, const phys_params* p, double* fx, double* fy, double* fz) {
+  if (!c) return PHYS_ERR_ARG;
+  PHYS_TRY(check_params(c, p));
+  if (!fx || !fy || !fz) return fail(c, PHYS_ERR_ARG, "force arrays are required");
+  int64_t n = c->n;
+  if (n < 2) return PHYS_OK;  // gravity.rs:49-51
+  PHYS_TRY(reset_status(c));
+  PHYS_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+  PHYS_TRY(eval(c, p, true));
+  PHYS_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+  PHYS_TRY(ensure_pinned(c, sizeof(double) * 3 * n));
+  double* h = static_cast<double*>(c->h_stage);
+  PHYS_TRY(d2h(c, h, c->fx, n));
+  PHYS_TRY(d2h(c, h + n, c->fy, n));
+  PHYS_TRY(d2h(c, h + 2 * n, c->fz, n));
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  int st = finish_status(c);
+  c->tm.total_ms = ev_ms(c->ev[0], c->ev[1]);
+  if (st) return st;
+  for (int64_t i = 0; i < n; ++i) {  // Force += computed (gravity.rs:71-73)
+    fx[i] += h[i];
+    fy[i] += h[n + i];
+    fz[i] += h[2 * n + i];
+  }
+  return PHYS_OK;
+}
+
+int phys_gravity_accel(phys_ctx* c, const phys_params* p, double* ax, double* ay, double* az) {
+  if (!c) return PHYS_ERR_ARG;
+  PHYS_TRY(check_params(c, p));
+  if (c->n == 0) return fail(c, PHYS_ERR_STATE, "no body state uploaded");
+  PHYS_TRY(reset_status(c));
+  PHYS_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+  PHYS_TRY(eval(c, p, false));
+  PHYS_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+  c->accel_valid = true;
+  c->accel_params = *p;
+  PHYS_TRY(d2h(c, ax, c->ax, c->n));
+  PHYS_TRY(d2h(c, ay, c->ay, c->n));
+  PHYS_TRY(d2h(c, az, c->az, c->n));
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  int st = finish_status(c);
+  c->tm.total_ms = ev_ms(c->ev[0], c->ev[1]);
+  return st;
+}
+
+int phys_verlet_steps(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps) {
+  if (!c) return PHYS_ERR_ARG;
+  return verlet_steps(c, p, dt, nsteps, true);
+}
+
+int phys_verlet_steps_async(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps) {
+  if (!c) return PHYS_ERR_ARG;
+  return verlet_steps(c, p, dt, nsteps, false);
+}
+
+int phys_diagnostics(phys_ctx* c, double G, double* out5) {
+  if (!c || !out5) return PHYS_ERR_ARG;
+  if (c->n == 0) return fail(c, PHYS_ERR_STATE, "no body state uploaded");
+  return diagnostics(c, G, out5);
+}
+
+int phys_bh_export(phys_ctx* c, const phys_params* p, int64_t cap, int64_t* nnodes,
+                   int32_t* depth, int64_t* count, double* mass, double* com,
+                   int64_t* leaf_body, int64_t* body_leaf, uint64_t* keys_hi, uint64_t* keys_lo,
+                   int64_t* perm, double* root4) {
+  if (!c) return PHYS_ERR_ARG;
+  PHYS_TRY(check_params(c, p));
+  if (c->n < 2) return fail(c, PHYS_ERR_STATE, "need at least 2 bodies");
+  if (cap < 0) return fail(c, PHYS_ERR_ARG, "cap < 0");
+  PHYS_TRY(reset_status(c));
+  PHYS_TRY(bh_export(c, p, cap, nnodes, depth, count, mass, com, leaf_body, body_leaf, keys_hi,
+                     keys_lo, perm, root4));
+  return finish_status(c);
+}
+
+int phys_probe_peaks(phys_ctx* c, double* fp32, double* fp64) {
+  if (!c || !fp32 || !fp64) return PHYS_ERR_ARG;
+  return probe_peaks(c, fp32, fp64);
+}
+
+}  // extern "C"

@@ -1,0 +1,339 @@
+// K1: softened all-pairs direct sum (brute_force_gravity_system,
+// src/physics/gravity.rs:53-69), in three precisions.
+//
+// Layout: sources are staged through shared memory in tiles; every lane of a
+// warp reads the same source (shared-memory broadcast) while owning one
+// target.  For small N the source range is split into `slices` so the grid
+// covers all SMs; slice partials are reduced in slice order (deterministic).
+#include "common.cuh"
+
+namespace phys {
+namespace {
+
+// ---------------------------------------------------------------------------
+// F64_EXACT: the reference's arithmetic, j in order 0..N-1, no FMA.
+//   r = x_j - x_i; r2 = len2(r); s2 = r2 + eps2; s3 = s2 * sqrt(s2)
+//   sc = ((G*m_i)*m_j)/s3; F += r*sc            (gravity.rs:58-65)
+// One thread per target; the j order fixes the summation, so no slicing.
+// ---------------------------------------------------------------------------
+constexpr int kExactBlock = 64;
+
+__global__ void __launch_bounds__(kExactBlock)
+direct_exact_kernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                    const double* __restrict__ z, const double* __restrict__ m, double G,
+                    double eps2, int want_force, double* __restrict__ ox,
+                    double* __restrict__ oy, double* __restrict__ oz, int32_t* status) {
+  __shared__ double4 tile[kExactBlock];
+  const int64_t i = blockIdx.x * (int64_t)kExactBlock + threadIdx.x;
+  const bool valid = i < n;
+  double xi = 0, yi = 0, zi = 0, mi = 0;
+  if (valid) {
+    xi = x[i];
+    yi = y[i];
+    zi = z[i];
+    mi = m[i];
+  }
+  const double gm = xmul(G, mi);
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  for (int64_t base = 0; base < n; base += kExactBlock) {
+    int64_t j = base + threadIdx.x;
+    __syncthreads();
+    tile[threadIdx.x] = j < n ? make_double4(x[j], y[j], z[j], m[j]) : make_double4(0, 0, 0, 0);
+    __syncthreads();
+    const int cnt = (int)min64(kExactBlock, n - base);
+    for (int k = 0; k < cnt; ++k) {
+      if (base + k == i) continue;
+      const double4 s = tile[k];
+      const double rx = xsub(s.x, xi), ry = xsub(s.y, yi), rz = xsub(s.z, zi);
+      const double r2 = xlen2(rx, ry, rz);
+      const double s2 = xadd(r2, eps2);
+      const double s3 = xmul(s2, xsqrt(s2));
+      const double sc = xdiv(xmul(gm, s.w), s3);
+      fx = xadd(fx, xmul(rx, sc));
+      fy = xadd(fy, xmul(ry, sc));
+      fz = xadd(fz, xmul(rz, sc));
+    }
+  }
+  if (valid) {
+    if (!want_force) {  // compute_acceleration_system: a = F / m (integrators.rs:115)
+      fx = xdiv(fx, mi);
+      fy = xdiv(fy, mi);
+      fz = xdiv(fz, mi);
+    }
+    ox[i] = fx;
+    oy[i] = fy;
+    oz[i] = fz;
+  }
+  bool bad = valid && (!isfinite(fx) || !isfinite(fy) || !isfinite(fz));
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(status, kStatNonfinite);
+}
+
+// ---------------------------------------------------------------------------
+// F64: same law with FMA and rsqrt, accumulating sum m_j r / s^3 (G applied
+// at the end).  Sources in [slice_lo, slice_hi); tile-aligned, so the tile
+// holding the block's own targets (the only one that can contain j == i) is
+// warp-uniform and takes the checked loop.
+// ---------------------------------------------------------------------------
+constexpr int kTile = 128;
+
+template <bool kChecked>
+__device__ __forceinline__ void f64_tile(const double4* __restrict__ t, int cnt, int self,
+                                         double xi, double yi, double zi, double eps2,
+                                         double& ax, double& ay, double& az) {
+#pragma unroll 4
+  for (int k = 0; k < cnt; ++k) {
+    const double4 s = t[k];
+    const double rx = s.x - xi, ry = s.y - yi, rz = s.z - zi;
+    double r2 = fma(rx, rx, fma(ry, ry, fma(rz, rz, eps2)));
+    double mj = s.w;
+    if (kChecked && k == self) {
+      mj = 0.0;
+      r2 = 1.0;
+    }
+    const double inv = rsqrt(r2);
+    const double w = mj * (inv * inv * inv);
+    ax = fma(rx, w, ax);
+    ay = fma(ry, w, ay);
+    az = fma(rz, w, az);
+  }
+}
+
+__global__ void __launch_bounds__(kTile)
+direct_f64_kernel(int64_t n, int64_t slice_len, const double* __restrict__ x,
+                  const double* __restrict__ y, const double* __restrict__ z,
+                  const double* __restrict__ m, double G, double eps2, int want_force,
+                  double* __restrict__ ox, double* __restrict__ oy, double* __restrict__ oz,
+                  double* __restrict__ part, int32_t* status) {
+  __shared__ double4 tile[kTile];
+  const int64_t tbase = blockIdx.x * (int64_t)kTile;
+  const int64_t i = tbase + threadIdx.x;
+  const bool valid = i < n;
+  const double xi = valid ? x[i] : 0.0, yi = valid ? y[i] : 0.0, zi = valid ? z[i] : 0.0;
+  const int64_t lo = blockIdx.y * slice_len;
+  const int64_t hi = min64(n, lo + slice_len);
+  double ax = 0.0, ay = 0.0, az = 0.0;
+  for (int64_t base = lo; base < hi; base += kTile) {
+    int64_t j = base + threadIdx.x;
+    __syncthreads();
+    tile[threadIdx.x] = j < hi ? make_double4(x[j], y[j], z[j], m[j]) : make_double4(0, 0, 0, 0);
+    __syncthreads();
+    const int cnt = (int)min64(kTile, hi - base);
+    if (base == tbase)
+      f64_tile<true>(tile, cnt, threadIdx.x, xi, yi, zi, eps2, ax, ay, az);
+    else
+      f64_tile<false>(tile, cnt, -1, xi, yi, zi, eps2, ax, ay, az);
+  }
+  if (!valid) return;
+  if (gridDim.y == 1) {
+    double s = want_force ? G * m[i] : G;
+    ox[i] = ax * s;
+    oy[i] = ay * s;
+    oz[i] = az * s;
+    if (!isfinite(ax) || !isfinite(ay) || !isfinite(az)) atomicOr(status, kStatNonfinite);
+  } else {
+    double* p = part + (size_t)blockIdx.y * 3 * n;
+    p[i] = ax;
+    p[n + i] = ay;
+    p[2 * n + i] = az;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// F32C: f32 pair terms.  Positions are double-float pairs (hi, lo); the
+// separation r = (hi_j - hi_i) + (lo_j - lo_i) keeps ~1e-7 relative accuracy
+// however close the pair is compared with |x|.  Each group of 32 terms is
+// summed in plain f32 and folded into a per-target (hi, lo) accumulator with
+// Knuth's two-sum.
+// ---------------------------------------------------------------------------
+__global__ void split_bodies_kernel(int64_t n, const double* __restrict__ x,
+                                    const double* __restrict__ y, const double* __restrict__ z,
+                                    const double* __restrict__ m, float4* __restrict__ bh,
+                                    float4* __restrict__ bl, int32_t* status) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float4 h, l;
+    split_df(x[i], h.x, l.x);
+    split_df(y[i], h.y, l.y);
+    split_df(z[i], h.z, l.z);
+    h.w = (float)m[i];
+    l.w = 0.f;
+    bh[i] = h;
+    bl[i] = l;
+    if (!isfinite(x[i]) || !isfinite(y[i]) || !isfinite(z[i]) || !isfinite(m[i]))
+      atomicOr(status, kStatNonfinite);
+  }
+}
+
+template <bool kChecked>
+__device__ __forceinline__ void f32_group(const float4* __restrict__ th,
+                                          const float4* __restrict__ tl, int k0, int k1, int self,
+                                          float xh, float yh, float zh, float xl, float yl,
+                                          float zl, float eps2, float& px, float& py,
+                                          float& pz) {
+#pragma unroll 8
+  for (int k = k0; k < k1; ++k) {
+    const float4 h = th[k];
+    const float4 l = tl[k];
+    const float rx = (h.x - xh) + (l.x - xl);
+    const float ry = (h.y - yh) + (l.y - yl);
+    const float rz = (h.z - zh) + (l.z - zl);
+    float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2)));
+    float mj = h.w;
+    if (kChecked && k == self) {
+      mj = 0.f;
+      r2 = 1.f;
+    }
+    const float inv = rsqrtf(r2);
+    const float w = mj * (inv * inv * inv);
+    px = fmaf(rx, w, px);
+    py = fmaf(ry, w, py);
+    pz = fmaf(rz, w, pz);
+  }
+}
+
+__global__ void __launch_bounds__(kTile)
+direct_f32c_kernel(int64_t n, int64_t slice_len, const float4* __restrict__ bh,
+                   const float4* __restrict__ bl, const double* __restrict__ m, double G,
+                   float eps2, int want_force, double* __restrict__ ox, double* __restrict__ oy,
+                   double* __restrict__ oz, double* __restrict__ part, int32_t* status) {
+  __shared__ float4 th[kTile];
+  __shared__ float4 tl[kTile];
+  const int64_t tbase = blockIdx.x * (int64_t)kTile;
+  const int64_t i = tbase + threadIdx.x;
+  const bool valid = i < n;
+  float4 hi4 = valid ? bh[i] : make_float4(0, 0, 0, 0);
+  float4 lo4 = valid ? bl[i] : make_float4(0, 0, 0, 0);
+  const int64_t lo = blockIdx.y * slice_len;
+  const int64_t hi = min64(n, lo + slice_len);
+  float ahx = 0.f, ahy = 0.f, ahz = 0.f, alx = 0.f, aly = 0.f, alz = 0.f;
+  for (int64_t base = lo; base < hi; base += kTile) {
+    int64_t j = base + threadIdx.x;
+    __syncthreads();
+    th[threadIdx.x] = j < hi ? bh[j] : make_float4(0, 0, 0, 0);
+    tl[threadIdx.x] = j < hi ? bl[j] : make_float4(0, 0, 0, 0);
+    __syncthreads();
+    const int cnt = (int)min64(kTile, hi - base);
+    const bool diag = base == tbase;
+    for (int k0 = 0; k0 < cnt; k0 += 32) {
+      const int k1 = min(cnt, k0 + 32);
+      float px = 0.f, py = 0.f, pz = 0.f;
+      if (diag)
+        f32_group<true>(th, tl, k0, k1, threadIdx.x, hi4.x, hi4.y, hi4.z, lo4.x, lo4.y, lo4.z,
+                        eps2, px, py, pz);
+      else
+        f32_group<false>(th, tl, k0, k1, -1, hi4.x, hi4.y, hi4.z, lo4.x, lo4.y, lo4.z, eps2, px,
+                         py, pz);
+      float s, e;
+      two_sum(ahx, px, s, e);
+      ahx = s;
+      alx += e;
+      two_sum(ahy, py, s, e);
+      ahy = s;
+      aly += e;
+      two_sum(ahz, pz, s, e);
+      ahz = s;
+      alz += e;
+    }
+  }
+  if (!valid) return;
+  const double ax = (double)ahx + (double)alx;
+  const double ay = (double)ahy + (double)aly;
+  const double az = (double)ahz + (double)alz;
+  if (gridDim.y == 1) {
+    double s = want_force ? G * m[i] : G;
+    ox[i] = ax * s;
+    oy[i] = ay * s;
+    oz[i] = az * s;
+    if (!isfinite(ax) || !isfinite(ay) || !isfinite(az)) atomicOr(status, kStatNonfinite);
+  } else {
+    double* p = part + (size_t)blockIdx.y * 3 * n;
+    p[i] = ax;
+    p[n + i] = ay;
+    p[2 * n + i] = az;
+  }
+}
+
+// Sum slice partials in slice order and apply G (and m_i for forces).
+__global__ void slice_reduce_kernel(int64_t n, int nslices, const double* __restrict__ part,
+                                    const double* __restrict__ m, double G, int want_force,
+                                    double* __restrict__ ox, double* __restrict__ oy,
+                                    double* __restrict__ oz, int32_t* status) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    for (int s = 0; s < nslices; ++s) {
+      const double* p = part + (size_t)s * 3 * n;
+      ax += p[i];
+      ay += p[n + i];
+      az += p[2 * n + i];
+    }
+    double sc = want_force ? G * m[i] : G;
+    ox[i] = ax * sc;
+    oy[i] = ay * sc;
+    oz[i] = az * sc;
+    if (!isfinite(ax) || !isfinite(ay) || !isfinite(az)) atomicOr(status, kStatNonfinite);
+  }
+}
+
+// Slices so that about two waves of 148 SMs x 2048 threads are resident;
+// every slice spans whole tiles.
+int64_t choose_slices(int64_t n) {
+  const int64_t want_threads = 148LL * 2048;
+  int64_t s = ceil_div(want_threads, ceil_div(n, kTile) * kTile);
+  int64_t max_s = ceil_div(n, kTile);
+  if (s > max_s) s = max_s;
+  if (s < 1) s = 1;
+  return s;
+}
+
+}  // namespace
+
+int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, double* oy,
+                double* oz) {
+  const int64_t n = c->n;
+  const double eps2 = p->eps * p->eps;
+  PHYS_CUDA(c, cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned long long), c->stream));
+  PHYS_CUDA(c, cudaEventRecord(c->ev[6], c->stream));
+  if (p->precision == PHYS_F64_EXACT) {
+    PHYS_LAUNCH(c, direct_exact_kernel, (int)ceil_div(n, kExactBlock), kExactBlock, 0, n, c->x,
+                c->y, c->z, c->m, p->G, eps2, (int)want_force, ox, oy, oz, c->d_status);
+  } else {
+    const int64_t slices = choose_slices(n);
+    const int64_t slice_len = ceil_div(ceil_div(n, slices), kTile) * kTile;
+    const int64_t nsl = ceil_div(n, slice_len);
+    double* part = nullptr;
+    int st = PHYS_OK;
+    if (nsl > 1) {
+      part = (double*)ws_get(c, WS_DIRECT_PART, sizeof(double) * 3 * n * nsl, &st);
+      if (st) return st;
+    }
+    dim3 grid((unsigned)ceil_div(n, kTile), (unsigned)nsl);
+    if (p->precision == PHYS_F64) {
+      PHYS_LAUNCH(c, direct_f64_kernel, grid, kTile, 0, n, slice_len, c->x, c->y, c->z, c->m, p->G,
+                  eps2, (int)want_force, ox, oy, oz, part, c->d_status);
+    } else {
+      float4* bh = (float4*)ws_get(c, WS_BODY_HI, sizeof(float4) * n, &st);
+      if (st) return st;
+      float4* bl = (float4*)ws_get(c, WS_BODY_LO, sizeof(float4) * n, &st);
+      if (st) return st;
+      int g = (int)min64(ceil_div(n, 256), 148 * 8);
+      PHYS_LAUNCH(c, split_bodies_kernel, g, 256, 0, n, c->x, c->y, c->z, c->m, bh, bl,
+                  c->d_status);
+      PHYS_LAUNCH(c, direct_f32c_kernel, grid, kTile, 0, n, slice_len, bh, bl, c->m, p->G,
+                  (float)eps2, (int)want_force, ox, oy, oz, part, c->d_status);
+    }
+    if (nsl > 1) {
+      int g = (int)min64(ceil_div(n, 256), 148 * 8);
+      PHYS_LAUNCH(c, slice_reduce_kernel, g, 256, 0, n, (int)nsl, part, c->m, p->G,
+                  (int)want_force, ox, oy, oz, c->d_status);
+    }
+  }
+  PHYS_CUDA(c, cudaEventRecord(c->ev[7], c->stream));
+  c->tm.interactions = (uint64_t)n * (uint64_t)(n - 1);
+  c->tm.bbox_ms = c->tm.keys_ms = c->tm.sort_ms = c->tm.tree_ms = 0.0;
+  c->tm.nodes = 0;
+  c->tm.max_depth = 0;
+  return PHYS_OK;
+}
+
+}  // namespace phys

@@ -1,0 +1,785 @@
+// Barnes-Hut octree build on the device: bounding cube (K2), descent keys
+// (K3), radix sort + equal-prefix fixup (K4), linear pre-order octree with
+// per-cell mass and centre of mass (K5).
+//
+// The tree equals the reference's (gravity_tree.rs:110-154 run over the
+// bodies in index order): a cell is split iff it holds >= 2 bodies and lies
+// above the guard depth D* (depth >= 40 or half size < 1e-8); a cell at D*
+// is a leaf that keeps the LAST inserted body while its mass and centre of
+// mass count all of them.  Cell boundaries are the reference's f64 centres
+// c +/- h/2 applied level by level, which the descent key reproduces bit for
+// bit: octant = (x >= cx) | (y >= cy) << 1 | (z >= cz) << 2 per level.
+//
+// Ownership rule used to emit nodes in pre-order without recursion: with
+// L[p] = common prefix length (octants, capped at D*) of sorted keys p, p+1
+// (L[-1] = L[n-1] = -1), sorted position p owns the cells that start at p:
+//   L[p-1] >= D*           -> none (inside a guard group)
+//   L[p]   >= D*           -> internal cells at depths L[p-1]+1 .. D*-1, guard leaf at D*
+//   otherwise              -> internal cells at depths L[p-1]+1 .. L[p],
+//                             leaf at max(L[p-1], L[p]) + 1
+// Pre-order = order of (start, depth), so node ids are a prefix sum.
+#include <vector>
+
+#include "bh.cuh"
+
+namespace phys {
+namespace {
+
+constexpr int kBlock = 256;
+
+int grid_for(int64_t n, int block = kBlock, int cap = 148 * 16) {
+  int64_t g = ceil_div(n, block);
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+// ---------------------------------------------------------------------------
+// K2: bounding cube, gravity_tree.rs:305-317.
+// ---------------------------------------------------------------------------
+constexpr int kBboxGrid = 296;
+
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__global__ void __launch_bounds__(kBlock)
+bbox_partial_kernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                    const double* __restrict__ z, const double* __restrict__ m,
+                    double* __restrict__ part, int32_t* status) {
+  __shared__ double sh[6][kBlock / 32];
+  double v[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+  bool bad = false;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double a = x[i], b = y[i], cc = z[i];
+    v[0] = fmin(v[0], a);
+    v[1] = fmin(v[1], b);
+    v[2] = fmin(v[2], cc);
+    v[3] = fmax(v[3], a);
+    v[4] = fmax(v[4], b);
+    v[5] = fmax(v[5], cc);
+    bad |= !isfinite(a) || !isfinite(b) || !isfinite(cc) || !isfinite(m[i]);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) v[k] = warp_min(v[k]);
+#pragma unroll
+  for (int k = 3; k < 6; ++k) v[k] = warp_max(v[k]);
+  if (lane == 0)
+    for (int k = 0; k < 6; ++k) sh[k][warp] = v[k];
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status, kStatNonfinite);
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      double t = lane < kBlock / 32 ? sh[k][lane] : (k < 3 ? INFINITY : -INFINITY);
+      t = k < 3 ? warp_min(t) : warp_max(t);
+      if (lane == 0) part[blockIdx.x * 6 + k] = t;
+    }
+  }
+}
+
+__global__ void bbox_final_kernel(int nparts, const double* __restrict__ part, double theta,
+                                  TreeHeader* hdr, const int32_t* status) {
+  if (threadIdx.x != 0) return;
+  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int b = 0; b < nparts; ++b)
+    for (int k = 0; k < 3; ++k) {
+      mn[k] = fmin(mn[k], part[b * 6 + k]);
+      mx[k] = fmax(mx[k], part[b * 6 + 3 + k]);
+    }
+  // extent = max - min; max_extent = x.max(y).max(z); half = max_extent*0.55 + 1
+  const double ex = xsub(mx[0], mn[0]), ey = xsub(mx[1], mn[1]), ez = xsub(mx[2], mn[2]);
+  const double max_extent = fmax(fmax(ex, ey), ez);
+  const double half = xadd(xmul(max_extent, 0.55), 1.0);
+  for (int k = 0; k < 3; ++k) hdr->center[k] = xmul(xadd(mn[k], mx[k]), 0.5);
+  hdr->half = half;
+  hdr->theta2 = xmul(theta, theta);
+  double h = half;
+  int dstar = -1;
+  for (int d = 0; d < kMaxLevels; ++d) {
+    const double s = xmul(h, 2.0);  // full side length (gravity_tree.rs:192)
+    hdr->s2[d] = xmul(s, s);
+    if (dstar < 0 && (d >= kMaxDepth || h < kMinNodeSize)) dstar = d;
+    h = xmul(h, 0.5);  // child half size (gravity_tree.rs:137)
+  }
+  hdr->dstar = dstar;
+  hdr->nonfinite = (*status & kStatNonfinite) ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// K3: descent keys.  hi = octants 0..20 (octant d in bits 62-3d..60-3d), lo =
+// octants 21..39 (bits 56..0); octants below D* are zero for every body.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock)
+keys_kernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+            const double* __restrict__ z, const TreeHeader* __restrict__ hdr,
+            uint64_t* __restrict__ khi, uint64_t* __restrict__ klo, uint32_t* __restrict__ idx) {
+  const double c0 = hdr->center[0], c1 = hdr->center[1], c2 = hdr->center[2];
+  const double h0 = hdr->half;
+  const int D = hdr->dstar;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double px = x[i], py = y[i], pz = z[i];
+    double cx = c0, cy = c1, cz = c2, h = h0;
+    uint64_t kh = 0, kl = 0;
+    for (int d = 0; d < D; ++d) {
+      const uint32_t o = (px >= cx ? 1u : 0u) | (py >= cy ? 2u : 0u) | (pz >= cz ? 4u : 0u);
+      const double q = xmul(h, 0.5);  // child_center, gravity_tree.rs:100-107
+      cx = xadd(cx, (o & 1u) ? q : -q);
+      cy = xadd(cy, (o & 2u) ? q : -q);
+      cz = xadd(cz, (o & 4u) ? q : -q);
+      h = q;
+      if (d < 21)
+        kh |= (uint64_t)o << (60 - 3 * d);
+      else
+        kl |= (uint64_t)o << (54 - 3 * (d - 21));
+    }
+    khi[i] = kh;
+    klo[i] = kl;
+    idx[i] = (uint32_t)i;
+  }
+}
+
+// Bodies whose first 21 octants agree are ordered by (lo, index) in place.
+// The radix pass over hi is stable on index-ordered input, so each run is
+// already in index order; runs are rare (cells of side 2h/2^21).
+__device__ __forceinline__ bool key_less(const uint64_t* klo, uint32_t a, uint32_t b) {
+  const uint64_t la = klo[a], lb = klo[b];
+  return la < lb || (la == lb && a < b);
+}
+
+__global__ void run_fixup_kernel(int64_t n, const uint64_t* __restrict__ hs,
+                                 uint32_t* __restrict__ perm, const uint64_t* __restrict__ klo,
+                                 uint32_t* __restrict__ tmp) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p + 1 < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t h = hs[p];
+    if (hs[p + 1] != h) continue;
+    if (p > 0 && hs[p - 1] == h) continue;
+    int64_t e = p + 2;
+    while (e < n && hs[e] == h) ++e;
+    const int64_t len = e - p;
+    uint32_t* a = perm + p;
+    if (len <= 32) {
+      for (int64_t i = 1; i < len; ++i) {
+        const uint32_t v = a[i];
+        int64_t j = i - 1;
+        while (j >= 0 && key_less(klo, v, a[j])) {
+          a[j + 1] = a[j];
+          --j;
+        }
+        a[j + 1] = v;
+      }
+    } else {  // bottom-up merge sort through tmp[p..e)
+      uint32_t* src = a;
+      uint32_t* dst = tmp + p;
+      for (int64_t w = 1; w < len; w *= 2) {
+        for (int64_t lo = 0; lo < len; lo += 2 * w) {
+          int64_t mid = min(lo + w, len), hi = min(lo + 2 * w, len);
+          int64_t i = lo, j = mid, k = lo;
+          while (i < mid && j < hi) dst[k++] = key_less(klo, src[j], src[i]) ? src[j++] : src[i++];
+          while (i < mid) dst[k++] = src[i++];
+          while (j < hi) dst[k++] = src[j++];
+        }
+        uint32_t* t = src;
+        src = dst;
+        dst = t;
+      }
+      if (src != a)
+        for (int64_t i = 0; i < len; ++i) a[i] = src[i];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBlock)
+gather_sorted_kernel(int64_t n, const uint32_t* __restrict__ perm, const uint64_t* __restrict__ klo,
+                     const double* __restrict__ x, const double* __restrict__ y,
+                     const double* __restrict__ z, const double* __restrict__ m,
+                     uint64_t* __restrict__ lo_s, double4* __restrict__ body64,
+                     float4* __restrict__ body_hi, float4* __restrict__ body_lo) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t i = perm[p];
+    lo_s[p] = klo[i];
+    const double4 b = make_double4(x[i], y[i], z[i], m[i]);
+    body64[p] = b;
+    if (body_hi) {
+      float4 h, l;
+      split_df(b.x, h.x, l.x);
+      split_df(b.y, h.y, l.y);
+      split_df(b.z, h.z, l.z);
+      h.w = (float)b.w;
+      l.w = 0.f;
+      body_hi[p] = h;
+      body_lo[p] = l;
+    }
+  }
+}
+
+__device__ __forceinline__ int lcp_octants(uint64_t ha, uint64_t la, uint64_t hb, uint64_t lb) {
+  if (ha != hb) return (__clzll((long long)(ha ^ hb)) - 1) / 3;
+  if (la != lb) return 21 + (__clzll((long long)(la ^ lb)) - 7) / 3;
+  return kMaxDepth;
+}
+
+__global__ void __launch_bounds__(kBlock)
+lcp_count_kernel(int64_t n, const uint64_t* __restrict__ hs, const uint64_t* __restrict__ ls,
+                 const TreeHeader* __restrict__ hdr, int32_t* __restrict__ L,
+                 int32_t* __restrict__ cnt) {
+  const int D = hdr->dstar;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p <= n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    if (p == n) {
+      cnt[n] = 0;
+      continue;
+    }
+    const int Ln = p + 1 < n ? min(lcp_octants(hs[p], ls[p], hs[p + 1], ls[p + 1]), D) : -1;
+    const int Lp = p > 0 ? min(lcp_octants(hs[p - 1], ls[p - 1], hs[p], ls[p]), D) : -1;
+    L[p] = Ln;
+    int c;
+    if (Lp >= D)
+      c = 0;
+    else if (Ln >= D)
+      c = D - Lp;
+    else
+      c = max(0, Ln - Lp) + 1;
+    cnt[p] = c;
+  }
+}
+
+// Keys truncated to the first d octants.
+__device__ __forceinline__ void trunc_key(uint64_t h, uint64_t l, int d, uint64_t& th,
+                                          uint64_t& tl) {
+  if (d <= 21) {
+    const uint64_t keep = (1ull << 63) - 1;
+    const uint64_t drop = d == 21 ? 0ull : ((1ull << (63 - 3 * d)) - 1);
+    th = h & (keep ^ drop);
+    tl = 0;
+  } else {
+    th = h;
+    const uint64_t keep = (1ull << 57) - 1;
+    const int dd = d - 21;
+    const uint64_t drop = dd >= 19 ? 0ull : ((1ull << (57 - 3 * dd)) - 1);
+    tl = l & (keep ^ drop);
+  }
+}
+
+// First q > p whose key differs from key p in the first d octants (n if none).
+__device__ int64_t cell_end(int64_t n, const uint64_t* __restrict__ hs,
+                            const uint64_t* __restrict__ ls, int64_t p, int d) {
+  uint64_t ph, pl;
+  trunc_key(hs[p], ls[p], d, ph, pl);
+  auto same = [&](int64_t q) {
+    uint64_t qh, ql;
+    trunc_key(hs[q], ls[q], d, qh, ql);
+    return qh == ph && ql == pl;
+  };
+  // gallop: find hi with !same(hi) or hi == n
+  int64_t lo = p + 1, step = 1, hi = p + 1;
+  while (hi < n && same(hi)) {
+    lo = hi + 1;
+    hi = p + 1 + step;
+    step <<= 1;
+    if (hi > n) hi = n;
+  }
+  // answer in [lo, hi]
+  while (lo < hi) {
+    const int64_t mid = lo + (hi - lo) / 2;
+    if (same(mid))
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kBlock)
+emit_nodes_kernel(int64_t n, const uint64_t* __restrict__ hs, const uint64_t* __restrict__ ls,
+                  const int32_t* __restrict__ L, const int32_t* __restrict__ cnt,
+                  const int32_t* __restrict__ first, const TreeHeader* __restrict__ hdr,
+                  int4* __restrict__ link) {
+  const int D = hdr->dstar;
+  const int32_t total = first[n];
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int c = cnt[p];
+    if (c == 0) continue;
+    const int32_t f = first[p];
+    const int Lp = p > 0 ? L[p - 1] : -1;
+    const int Ln = L[p];
+    const bool guard = Ln >= D;
+    for (int k = 0; k < c; ++k) {
+      const int d = Lp + 1 + k;
+      const bool leaf = k == c - 1;
+      int64_t end;
+      if (leaf && !guard)
+        end = p + 1;
+      else
+        end = cell_end(n, hs, ls, p, d);
+      const int32_t next = end < n ? first[end] : total;
+      int meta = d;
+      if (leaf) meta |= kMetaLeaf;
+      if (leaf && guard) meta |= kMetaGuard;
+      link[f + k] = make_int4(next, (int)p, (int)end, meta);
+    }
+  }
+}
+
+// parent / number of children, by walking each internal node's child chain.
+__global__ void __launch_bounds__(kBlock)
+children_kernel(int64_t nnodes, const int4* __restrict__ link, int32_t* __restrict__ parent,
+                int32_t* __restrict__ nchild, int32_t* status) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnodes;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int4 lk = link[k];
+    if (k == 0) parent[0] = -1;
+    int cc = 0;
+    if (!(lk.w & kMetaLeaf)) {
+      int32_t ch = (int32_t)k + 1;
+      while (ch < lk.x && cc < 8) {  // an octree cell has at most 8 children
+        parent[ch] = (int32_t)k;
+        const int32_t nx = link[ch].x;
+        if (nx <= ch) break;
+        ch = nx;
+        ++cc;
+      }
+      if (ch < lk.x) atomicOr(status, kStatOverflow);
+    }
+    nchild[k] = cc;
+  }
+}
+
+// Bucket leaves: keep a node iff its parent holds more than `cap` bodies.
+__global__ void keep_kernel(int64_t nnodes, const int4* __restrict__ link,
+                            const int32_t* __restrict__ parent, int cap,
+                            int32_t* __restrict__ keep) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k <= nnodes;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    if (k == nnodes) {
+      keep[k] = 0;
+      continue;
+    }
+    if (k == 0) {
+      keep[0] = 1;
+      continue;
+    }
+    const int4 pl = link[parent[k]];
+    keep[k] = (pl.z - pl.y) > cap ? 1 : 0;
+  }
+}
+
+__global__ void compact_kernel(int64_t nnodes, const int4* __restrict__ link,
+                               const int32_t* __restrict__ keep, const int32_t* __restrict__ newid,
+                               int cap, int4* __restrict__ out) {
+  const int32_t total = newid[nnodes];
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnodes;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    if (!keep[k]) continue;
+    const int4 lk = link[k];
+    const int32_t nx = lk.x >= nnodes ? total : newid[lk.x];
+    int meta = lk.w;
+    if ((lk.z - lk.y) <= cap) meta |= kMetaLeaf;
+    out[newid[k]] = make_int4(nx, lk.y, lk.z, meta);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Mass / centre of mass, parallel form: sums of m and m*x, leaves over their
+// bodies in key order, internal cells over their children in octant order
+// (fixed order: deterministic), propagated bottom-up by the last-arriving
+// child.  Differs from the reference's insertion-order running mean by ulps.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock)
+com_upward_kernel(int64_t nnodes, const int4* __restrict__ link,
+                  const int32_t* __restrict__ parent, const int32_t* __restrict__ nchild,
+                  int32_t* __restrict__ arrive, const double4* __restrict__ body64,
+                  double4* __restrict__ sums, int32_t* status) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnodes;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int4 lk = link[k];
+    if (!(lk.w & kMetaLeaf)) continue;
+    double sx = 0.0, sy = 0.0, sz = 0.0, sm = 0.0;
+    for (int q = lk.y; q < lk.z; ++q) {
+      const double4 b = body64[q];
+      sx = fma(b.w, b.x, sx);
+      sy = fma(b.w, b.y, sy);
+      sz = fma(b.w, b.z, sz);
+      sm += b.w;
+    }
+    sums[k] = make_double4(sx, sy, sz, sm);
+    int32_t cur = (int32_t)k;
+    while (cur != 0) {
+      __threadfence();
+      const int32_t par = parent[cur];
+      if (par < 0 || par >= cur) {  // parents precede children in pre-order
+        atomicOr(status, kStatOverflow);
+        break;
+      }
+      if (atomicAdd(&arrive[par], 1) != nchild[par] - 1) break;
+      __threadfence();
+      const int32_t stop = link[par].x;
+      double ax = 0.0, ay = 0.0, az = 0.0, am = 0.0;
+      int guard = 0;
+      for (int32_t ch = par + 1; ch < stop && guard < 8; ch = link[ch].x, ++guard) {
+        const double2* sp = reinterpret_cast<const double2*>(&sums[ch]);
+        const double2 v0 = __ldcg(sp), v1 = __ldcg(sp + 1);  // L2: written by other threads
+        ax += v0.x;
+        ay += v0.y;
+        az += v1.x;
+        am += v1.y;
+      }
+      sums[par] = make_double4(ax, ay, az, am);
+      cur = par;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Mass / centre of mass, reference form (gravity_tree.rs:113-118): for every
+// cell the running mean com = (com*M + p*m) / (M + m) over its bodies in
+// index (insertion) order.  Segments (node, body) pairs sorted by node then
+// index, then one thread per node runs the recurrence.
+// ---------------------------------------------------------------------------
+__global__ void node_count_kernel(int64_t nnodes, const int4* __restrict__ link,
+                                  int32_t* __restrict__ cnt) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k <= nnodes;
+       k += (int64_t)gridDim.x * blockDim.x)
+    cnt[k] = k < nnodes ? link[k].z - link[k].y : 0;
+}
+
+__global__ void __launch_bounds__(kBlock)
+expand_kernel(int64_t total, int64_t nnodes, const int32_t* __restrict__ eoff,
+              const int4* __restrict__ link, const uint32_t* __restrict__ perm,
+              uint64_t* __restrict__ entries) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo = 0, hi = nnodes;  // last k with eoff[k] <= e
+    while (hi - lo > 1) {
+      const int64_t mid = (lo + hi) / 2;
+      if (eoff[mid] <= e)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const int q = link[lo].y + (int)(e - eoff[lo]);
+    entries[e] = ((uint64_t)lo << 32) | perm[q];
+  }
+}
+
+__global__ void __launch_bounds__(kBlock)
+com_recurrence_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
+                      const uint64_t* __restrict__ entries, const double* __restrict__ x,
+                      const double* __restrict__ y, const double* __restrict__ z,
+                      const double* __restrict__ m, double4* __restrict__ mc) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnodes;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e0 = eoff[k], e1 = eoff[k + 1];
+    double M = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
+    constexpr int kB = 8;
+    for (int64_t e = e0; e < e1; e += kB) {
+      double bx[kB], by[kB], bz[kB], bm[kB];
+#pragma unroll
+      for (int u = 0; u < kB; ++u) {
+        if (e + u < e1) {
+          const uint32_t b = (uint32_t)(entries[e + u] & 0xffffffffu);
+          bx[u] = x[b];
+          by[u] = y[b];
+          bz[u] = z[b];
+          bm[u] = m[b];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kB; ++u) {
+        if (e + u < e1) {
+          const double nt = xadd(M, bm[u]);
+          if (nt > 0.0) {
+            cx = xdiv(xadd(xmul(cx, M), xmul(bx[u], bm[u])), nt);
+            cy = xdiv(xadd(xmul(cy, M), xmul(by[u], bm[u])), nt);
+            cz = xdiv(xadd(xmul(cz, M), xmul(bz[u], bm[u])), nt);
+          }
+          M = nt;
+        }
+      }
+    }
+    mc[k] = make_double4(cx, cy, cz, M);
+  }
+}
+
+// Walk records + gate bit.  `mc` holds either raw sums (parallel form, turned
+// into com = S/M here) or finished (com, M) (reference form).
+__global__ void __launch_bounds__(kBlock)
+finalize_kernel(int64_t nnodes, int4* __restrict__ link, double4* __restrict__ mc, int sums,
+                int leaf_cap, const double4* __restrict__ body64, double4* __restrict__ rec64,
+                float4* __restrict__ rec_hi, float4* __restrict__ rec_lo) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnodes;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    int4 lk = link[k];
+    double4 a = mc[k];
+    if (sums) {
+      const double M = a.w;
+      if (M > 0.0)
+        a = make_double4(a.x / M, a.y / M, a.z / M, M);
+      else
+        a = make_double4(0.0, 0.0, 0.0, M);
+      mc[k] = a;
+    }
+    if (a.w > 0.0) lk.w |= kMetaGate;
+    link[k].w = lk.w;
+    double4 r = a;
+    if (lk.w & kMetaLeaf) {
+      const int cntb = lk.z - lk.y;
+      if (cntb == 1)
+        r = body64[lk.y];
+      else if ((lk.w & kMetaGuard) && leaf_cap == 1)
+        r = body64[lk.z - 1];  // the last inserted (highest index) body
+    }
+    if (rec64) rec64[k] = r;
+    if (rec_hi) {
+      float4 h, l;
+      split_df(r.x, h.x, l.x);
+      split_df(r.y, h.y, l.y);
+      split_df(r.z, h.z, l.z);
+      h.w = (float)r.w;
+      l.w = 0.f;
+      rec_hi[k] = h;
+      rec_lo[k] = l;
+    }
+  }
+}
+
+}  // namespace
+
+// Builds the tree for the current positions.  One host synchronisation reads
+// the node count (two with bucket leaves).
+int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t) {
+  const int64_t n = c->n;
+  const bool exact = p->precision == PHYS_F64_EXACT;
+  int st = PHYS_OK;
+#define WS(T, slot, count) (T*)ws_get(c, slot, sizeof(T) * (size_t)(count), &st); if (st) return st
+  uint64_t* khi = WS(uint64_t, WS_KEYS_HI, n);
+  uint64_t* klo = WS(uint64_t, WS_KEYS_LO, n);
+  uint32_t* idx = WS(uint32_t, WS_IDX, n);
+  uint64_t* khi_alt = WS(uint64_t, WS_KEYS_HI_ALT, n);
+  uint32_t* idx_alt = WS(uint32_t, WS_IDX_ALT, n);
+  uint64_t* lo_s = WS(uint64_t, WS_ENS7, n);
+  double4* body64 = WS(double4, WS_BODY_PM, n);
+  float4* body_hi = nullptr;
+  float4* body_lo = nullptr;
+  if (need_f32) {
+    body_hi = WS(float4, WS_BODY_HI, n);
+    body_lo = WS(float4, WS_BODY_LO, n);
+  }
+  int32_t* L = WS(int32_t, WS_LCP, n + 1);
+  int32_t* cnt = WS(int32_t, WS_NCOUNT, n + 1);
+  int32_t* first = WS(int32_t, WS_NFIRST, n + 1);
+  if (!c->d_partials || c->partials_cap < 6 * kBboxGrid) {
+    if (c->d_partials) cudaFree(c->d_partials);
+    c->d_partials = nullptr;
+    PHYS_CUDA(c, cudaMalloc(&c->d_partials, sizeof(double) * 8 * kBboxGrid));
+    c->partials_cap = 8 * kBboxGrid;
+  }
+
+  PHYS_CUDA(c, cudaEventRecord(c->ev[2], c->stream));
+  PHYS_LAUNCH(c, bbox_partial_kernel, kBboxGrid, kBlock, 0, n, c->x, c->y, c->z, c->m,
+              c->d_partials, c->d_status);
+  PHYS_LAUNCH(c, bbox_final_kernel, 1, 32, 0, kBboxGrid, c->d_partials, p->theta, c->d_hdr,
+              c->d_status);
+  PHYS_CUDA(c, cudaEventRecord(c->ev[3], c->stream));
+  PHYS_LAUNCH(c, keys_kernel, grid_for(n), kBlock, 0, n, c->x, c->y, c->z, c->d_hdr, khi, klo, idx);
+  PHYS_CUDA(c, cudaEventRecord(c->ev[4], c->stream));
+  bool in_alt = false;
+  PHYS_TRY(radix_sort_u64(c, khi, idx, khi_alt, idx_alt, n, 0, 64, &in_alt));
+  uint64_t* hs = in_alt ? khi_alt : khi;
+  uint32_t* perm = in_alt ? idx_alt : idx;
+  uint32_t* spare = in_alt ? idx : idx_alt;
+  PHYS_LAUNCH(c, run_fixup_kernel, grid_for(n), kBlock, 0, n, hs, perm, klo, spare);
+  PHYS_LAUNCH(c, gather_sorted_kernel, grid_for(n), kBlock, 0, n, perm, klo, c->x, c->y, c->z,
+              c->m, lo_s, body64, body_hi, body_lo);
+  PHYS_CUDA(c, cudaEventRecord(c->ev[5], c->stream));
+  PHYS_LAUNCH(c, lcp_count_kernel, grid_for(n + 1), kBlock, 0, n, hs, lo_s, c->d_hdr, L, cnt);
+  PHYS_TRY(scan_exclusive_i32(c, cnt, first, n + 1));
+  // node count + header back to the host
+  int32_t* hsm = c->h_small;
+  PHYS_CUDA(c, cudaMemcpyAsync(hsm, first + n, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  PHYS_CUDA(c, cudaMemcpyAsync(hsm + 1, &c->d_hdr->dstar, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                               c->stream));
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  int64_t nfull = hsm[0];
+  const int dstar = hsm[1];
+  if (nfull < 1 || nfull > (int64_t)n * (kMaxLevels + 1))
+    return fail(c, PHYS_ERR_CUDA, "tree build produced %lld nodes for %lld bodies",
+                (long long)nfull, (long long)n);
+  int4* link_full = WS(int4, WS_LINK2, nfull);
+  int32_t* parent = WS(int32_t, WS_PARENT, nfull + 1);
+  int32_t* nchild = WS(int32_t, WS_ARRIVE, 2 * (nfull + 1));
+  int32_t* arrive = nchild + (nfull + 1);
+  PHYS_LAUNCH(c, emit_nodes_kernel, grid_for(n), kBlock, 0, n, hs, lo_s, L, cnt, first, c->d_hdr,
+              link_full);
+  int4* link = link_full;
+  int64_t nnodes = nfull;
+  if (p->leaf_cap > 1) {
+    PHYS_LAUNCH(c, children_kernel, grid_for(nfull), kBlock, 0, nfull, link_full, parent, nchild,
+                c->d_status);
+    int32_t* keep = WS(int32_t, WS_KEEP, nfull + 1);
+    int32_t* newid = WS(int32_t, WS_NEWID, nfull + 1);
+    PHYS_LAUNCH(c, keep_kernel, grid_for(nfull + 1), kBlock, 0, nfull, link_full, parent,
+                p->leaf_cap, keep);
+    PHYS_TRY(scan_exclusive_i32(c, keep, newid, nfull + 1));
+    PHYS_CUDA(c, cudaMemcpyAsync(hsm, newid + nfull, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                 c->stream));
+    PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+    nnodes = hsm[0];
+    link = WS(int4, WS_LINK, nnodes);
+    PHYS_LAUNCH(c, compact_kernel, grid_for(nfull), kBlock, 0, nfull, link_full, keep, newid,
+                p->leaf_cap, link);
+  }
+  PHYS_LAUNCH(c, children_kernel, grid_for(nnodes), kBlock, 0, nnodes, link, parent, nchild,
+              c->d_status);
+  double4* mc = WS(double4, WS_NODE_S, nnodes);
+  if (exact) {
+    int32_t* ncnt = WS(int32_t, WS_KEEP, nnodes + 1);
+    int32_t* eoff = WS(int32_t, WS_EOFF, nnodes + 1);
+    PHYS_LAUNCH(c, node_count_kernel, grid_for(nnodes + 1), kBlock, 0, nnodes, link, ncnt);
+    PHYS_TRY(scan_exclusive_i32(c, ncnt, eoff, nnodes + 1));
+    PHYS_CUDA(c, cudaMemcpyAsync(hsm, eoff + nnodes, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                 c->stream));
+    PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+    const int64_t total = (uint32_t)hsm[0];
+    if (total <= 0 || total >= (int64_t(1) << 31))
+      return fail(c, PHYS_ERR_ARG, "exact centre of mass needs < 2^31 (cell, body) pairs");
+    uint64_t* ent = WS(uint64_t, WS_ENTRIES, total);
+    uint64_t* ent_alt = WS(uint64_t, WS_ENTRIES_ALT, total);
+    PHYS_LAUNCH(c, expand_kernel, grid_for(total), kBlock, 0, total, nnodes, eoff, link, perm, ent);
+    int bits_b = 1, bits_n = 1;
+    while ((int64_t(1) << bits_b) < n) ++bits_b;
+    while ((int64_t(1) << bits_n) < nnodes) ++bits_n;
+    bool alt1 = false, alt2 = false;
+    PHYS_TRY(radix_sort_u64(c, ent, nullptr, ent_alt, nullptr, total, 0, bits_b, &alt1));
+    uint64_t* e1 = alt1 ? ent_alt : ent;
+    uint64_t* e1_alt = alt1 ? ent : ent_alt;
+    PHYS_TRY(radix_sort_u64(c, e1, nullptr, e1_alt, nullptr, total, 32, 32 + bits_n, &alt2));
+    uint64_t* es = alt2 ? e1_alt : e1;
+    PHYS_LAUNCH(c, com_recurrence_kernel, grid_for(nnodes, 128, 1 << 30), 128, 0, nnodes, eoff, es,
+                c->x, c->y, c->z, c->m, mc);
+  } else {
+    PHYS_CUDA(c, cudaMemsetAsync(arrive, 0, sizeof(int32_t) * (nnodes + 1), c->stream));
+    PHYS_LAUNCH(c, com_upward_kernel, grid_for(nnodes), kBlock, 0, nnodes, link, parent, nchild,
+                arrive, body64, mc, c->d_status);
+  }
+  double4* rec64 = nullptr;
+  float4 *rec_hi = nullptr, *rec_lo = nullptr;
+  if (!need_f32) {
+    rec64 = WS(double4, WS_NODE_PM, nnodes);
+  } else {
+    rec_hi = WS(float4, WS_NODE_HI, nnodes);
+    rec_lo = WS(float4, WS_NODE_LO, nnodes);
+  }
+  PHYS_LAUNCH(c, finalize_kernel, grid_for(nnodes), kBlock, 0, nnodes, link, mc, exact ? 0 : 1,
+              p->leaf_cap, body64, rec64, rec_hi, rec_lo);
+#undef WS
+  t->n = n;
+  t->nnodes = nnodes;
+  t->leaf_cap = p->leaf_cap;
+  t->link = link;
+  t->rec64 = rec64;
+  t->rec_hi = rec_hi;
+  t->rec_lo = rec_lo;
+  t->mc = mc;
+  t->perm = perm;
+  t->body64 = body64;
+  t->body_hi = body_hi;
+  t->body_lo = body_lo;
+  t->hdr = c->d_hdr;
+  t->keys_hi_sorted = hs;
+  t->keys_lo = klo;
+  c->tm.nodes = nnodes;
+  c->tm.max_depth = dstar;
+  return PHYS_OK;
+}
+
+int bh_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, double* oy,
+            double* oz) {
+  BhTree t;
+  PHYS_TRY(bh_build(c, p, p->precision == PHYS_F32C, &t));
+  return bh_walk(c, p, t, want_force, ox, oy, oz);
+}
+
+int bh_export(phys_ctx* c, const phys_params* p, int64_t cap, int64_t* nnodes, int32_t* depth,
+              int64_t* count, double* mass, double* com, int64_t* leaf_body, int64_t* body_leaf,
+              uint64_t* keys_hi, uint64_t* keys_lo, int64_t* perm_out, double* root4) {
+  BhTree t;
+  PHYS_TRY(bh_build(c, p, false, &t));
+  const int64_t n = c->n, nn = t.nnodes;
+  std::vector<int4> link(nn);
+  std::vector<double4> mc(nn);
+  std::vector<uint32_t> perm(n);
+  TreeHeader hdr;
+  PHYS_CUDA(c, cudaMemcpyAsync(link.data(), t.link, sizeof(int4) * nn, cudaMemcpyDeviceToHost,
+                               c->stream));
+  PHYS_CUDA(c, cudaMemcpyAsync(mc.data(), t.mc, sizeof(double4) * nn, cudaMemcpyDeviceToHost,
+                               c->stream));
+  PHYS_CUDA(c, cudaMemcpyAsync(perm.data(), t.perm, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost,
+                               c->stream));
+  PHYS_CUDA(c, cudaMemcpyAsync(&hdr, t.hdr, sizeof(TreeHeader), cudaMemcpyDeviceToHost, c->stream));
+  std::vector<uint64_t> hs(keys_hi ? n : 0);
+  if (keys_hi)
+    PHYS_CUDA(c, cudaMemcpyAsync(hs.data(), t.keys_hi_sorted, sizeof(uint64_t) * n,
+                                 cudaMemcpyDeviceToHost, c->stream));
+  if (keys_lo)
+    PHYS_CUDA(c, cudaMemcpyAsync(keys_lo, t.keys_lo, sizeof(uint64_t) * n, cudaMemcpyDeviceToHost,
+                                 c->stream));
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (keys_hi)  // the sort reordered hi; undo it through the permutation
+    for (int64_t q = 0; q < n; ++q) keys_hi[perm[q]] = hs[q];
+  if (nnodes) *nnodes = nn;
+  if (root4) {
+    root4[0] = hdr.center[0];
+    root4[1] = hdr.center[1];
+    root4[2] = hdr.center[2];
+    root4[3] = hdr.half;
+  }
+  if (perm_out)
+    for (int64_t q = 0; q < n; ++q) perm_out[q] = perm[q];
+  if (body_leaf)
+    for (int64_t i = 0; i < n; ++i) body_leaf[i] = -1;
+  for (int64_t k = 0; k < nn; ++k) {
+    const int4 lk = link[k];
+    const bool leaf = lk.w & kMetaLeaf;
+    if (k < cap) {
+      if (depth) depth[k] = lk.w & kMetaDepth;
+      if (count) count[k] = lk.z - lk.y;
+      if (mass) mass[k] = mc[k].w;
+      if (com) {
+        com[3 * k] = mc[k].x;
+        com[3 * k + 1] = mc[k].y;
+        com[3 * k + 2] = mc[k].z;
+      }
+      if (leaf_body) {
+        int64_t lb = -1;
+        if (leaf) {
+          if (lk.z - lk.y == 1)
+            lb = perm[lk.y];
+          else if ((lk.w & kMetaGuard) && t.leaf_cap == 1)
+            lb = perm[lk.z - 1];
+          else
+            lb = -2;  // bucket leaf holding several bodies
+        }
+        leaf_body[k] = lb;
+      }
+    }
+    if (leaf && body_leaf)
+      for (int q = lk.y; q < lk.z; ++q) body_leaf[perm[q]] = k;
+  }
+  return PHYS_OK;
+}
+
+}  // namespace phys

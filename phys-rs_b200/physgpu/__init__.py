@@ -1,0 +1,448 @@
+"""physgpu: Python binding of libphysgpu.so (the B200 gravity library).
+
+Two layers:
+
+* `Context` wraps the C ABI of include/physgpu.h one call per method.
+* A mirror of the reference's gravity "plugin API" (bevy_ecs systems over
+  components, src/physics/*.rs): `UniverseConfig`, `SimulationTime`, a
+  structure-of-arrays `World`, and the systems
+  `brute_force_gravity_system`, `barnes_hut_gravity_system`,
+  `compute_acceleration_system`, `velocity_verlet_position_system`,
+  `velocity_verlet_velocity_system`, `reset_forces`, plus the energy systems.
+  Tests written against these read like the reference's own unit tests.
+
+There is no CPU fallback: importing works without a GPU, but any compute call
+raises `PhysError` when the CUDA library or a device is missing.
+"""
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG, "lib", "libphysgpu.so")
+
+OK, ERR_ARG, ERR_CUDA, ERR_OOM, ERR_NONFINITE, ERR_TIMEOUT, ERR_STATE = range(7)
+DIRECT, BARNES_HUT = 0, 1
+F64_EXACT, F64, F32C = 0, 1, 2
+COMP_POSITION, COMP_VELOCITY, COMP_ACCELERATION, COMP_PREV_ACCELERATION, COMP_MASS = range(5)
+
+PRECISIONS = {"f64_exact": F64_EXACT, "f64": F64, "f32c": F32C}
+
+# Every symbol include/physgpu.h declares.
+EXPORTED = [
+    "phys_status_string", "phys_last_error", "phys_ctx_create", "phys_ctx_destroy",
+    "phys_ctx_stream", "phys_last_timings", "phys_state_upload", "phys_state_upload_sectors",
+    "phys_state_set_accel", "phys_state_download", "phys_state_size", "phys_component_write",
+    "phys_component_read", "phys_gravity_forces", "phys_gravity_accel", "phys_verlet_steps",
+    "phys_vv_position_step", "phys_vv_velocity_step", "phys_verlet_steps_async",
+    "phys_diagnostics", "phys_bh_export", "phys_probe_peaks",
+]
+
+
+class PhysError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s (status %d)" % (msg, status))
+        self.status = status
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("G", ctypes.c_double), ("eps", ctypes.c_double), ("theta", ctypes.c_double),
+                ("method", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("leaf_cap", ctypes.c_int32), ("flags", ctypes.c_int32)]
+
+
+class Timings(ctypes.Structure):
+    _fields_ = [("total_ms", ctypes.c_double), ("bbox_ms", ctypes.c_double),
+                ("keys_ms", ctypes.c_double), ("sort_ms", ctypes.c_double),
+                ("tree_ms", ctypes.c_double), ("walk_ms", ctypes.c_double),
+                ("verlet_ms", ctypes.c_double), ("interactions", ctypes.c_uint64),
+                ("launches", ctypes.c_uint64), ("nodes", ctypes.c_int64),
+                ("max_depth", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+_lib = None
+_D = ctypes.POINTER(ctypes.c_double)
+_I64 = ctypes.POINTER(ctypes.c_int64)
+_I32 = ctypes.POINTER(ctypes.c_int32)
+_U64 = ctypes.POINTER(ctypes.c_uint64)
+_VP = ctypes.c_void_p
+
+
+def load_library(path=None):
+    """Load libphysgpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise PhysError(ERR_STATE, "libphysgpu.so not built (%s); run __graft_entry__.build()" % path)
+    L = ctypes.CDLL(path)
+    i32, i64, dbl = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+    P = ctypes.POINTER(Params)
+    sig = {
+        "phys_status_string": ([ctypes.c_int], ctypes.c_char_p),
+        "phys_last_error": ([_VP], ctypes.c_char_p),
+        "phys_ctx_create": ([ctypes.c_int, ctypes.POINTER(_VP)], ctypes.c_int),
+        "phys_ctx_destroy": ([_VP], ctypes.c_int),
+        "phys_ctx_stream": ([_VP], _VP),
+        "phys_last_timings": ([_VP, ctypes.POINTER(Timings)], ctypes.c_int),
+        "phys_state_upload": ([_VP, i64] + [_D] * 7, ctypes.c_int),
+        "phys_state_upload_sectors": ([_VP, i64, _I64, _I64, _I64, _D, _D, _D, dbl, i32]
+                                      + [_D] * 4, ctypes.c_int),
+        "phys_state_set_accel": ([_VP, _D, _D, _D], ctypes.c_int),
+        "phys_state_download": ([_VP] + [_D] * 9, ctypes.c_int),
+        "phys_state_size": ([_VP], i64),
+        "phys_component_write": ([_VP, i32, _D, _D, _D], ctypes.c_int),
+        "phys_component_read": ([_VP, i32, _D, _D, _D], ctypes.c_int),
+        "phys_gravity_forces": ([_VP, P, _D, _D, _D], ctypes.c_int),
+        "phys_gravity_accel": ([_VP, P, _D, _D, _D], ctypes.c_int),
+        "phys_verlet_steps": ([_VP, P, dbl, i64], ctypes.c_int),
+        "phys_verlet_steps_async": ([_VP, P, dbl, i64], ctypes.c_int),
+        "phys_vv_position_step": ([_VP, dbl], ctypes.c_int),
+        "phys_vv_velocity_step": ([_VP, dbl], ctypes.c_int),
+        "phys_diagnostics": ([_VP, dbl, _D], ctypes.c_int),
+        "phys_bh_export": ([_VP, P, i64, _I64, _I32, _I64, _D, _D, _I64, _I64, _U64, _U64, _I64,
+                            _D], ctypes.c_int),
+        "phys_probe_peaks": ([_VP, _D, _D], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _p(a, ty=_D):
+    return None if a is None else a.ctypes.data_as(ty)
+
+
+def _col(a, k):
+    return np.ascontiguousarray(a[:, k], dtype=np.float64)
+
+
+def make_params(G, eps, theta=0.5, method=DIRECT, precision=F64_EXACT, leaf_cap=1):
+    if isinstance(precision, str):
+        precision = PRECISIONS[precision]
+    return Params(float(G), float(eps), float(theta), int(method), int(precision), int(leaf_cap), 0)
+
+
+class Context:
+    """One device context: a CUDA stream plus device-resident body state."""
+
+    def __init__(self, device=0):
+        self.lib = load_library()
+        h = _VP()
+        st = self.lib.phys_ctx_create(int(device), ctypes.byref(h))
+        if st != OK:
+            raise PhysError(st, "phys_ctx_create(%d) failed: %s" % (
+                device, self.lib.phys_status_string(st).decode()))
+        self.h = h
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.phys_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st, what):
+        if st != OK:
+            raise PhysError(st, "%s: %s" % (what, self.lib.phys_last_error(self.h).decode()))
+
+    @property
+    def stream(self):
+        return self.lib.phys_ctx_stream(self.h)
+
+    # ---- state ----
+    def upload(self, pos, vel, m):
+        pos = np.asarray(pos, dtype=np.float64)
+        m = np.ascontiguousarray(m, dtype=np.float64)
+        n = m.shape[0]
+        P = [_col(pos, k) for k in range(3)]
+        V = [None] * 3 if vel is None else [_col(np.asarray(vel, np.float64), k) for k in range(3)]
+        self._check(self.lib.phys_state_upload(self.h, n, *[_p(a) for a in P],
+                                               *[_p(a) for a in V], _p(m)), "phys_state_upload")
+        self.n = n
+
+    def upload_sectors(self, sectors, local, sector_size, m, vel=None, bh_quirk=False):
+        s = np.ascontiguousarray(sectors, dtype=np.int64)
+        local = np.asarray(local, dtype=np.float64)
+        m = np.ascontiguousarray(m, dtype=np.float64)
+        n = m.shape[0]
+        S = [np.ascontiguousarray(s[:, k]) for k in range(3)]
+        Lc = [_col(local, k) for k in range(3)]
+        V = [None] * 3 if vel is None else [_col(np.asarray(vel, np.float64), k) for k in range(3)]
+        self._check(self.lib.phys_state_upload_sectors(
+            self.h, n, *[_p(a, _I64) for a in S], *[_p(a) for a in Lc], float(sector_size),
+            int(bool(bh_quirk)), *[_p(a) for a in V], _p(m)), "phys_state_upload_sectors")
+        self.n = n
+
+    def set_accel(self, acc):
+        A = [_col(np.asarray(acc, np.float64), k) for k in range(3)]
+        self._check(self.lib.phys_state_set_accel(self.h, *[_p(a) for a in A]),
+                    "phys_state_set_accel")
+
+    def download(self):
+        n = self.n
+        out = [np.empty(n) for _ in range(9)]
+        self._check(self.lib.phys_state_download(self.h, *[_p(a) for a in out]),
+                    "phys_state_download")
+        st = lambda a, b, c: np.stack([a, b, c], axis=1)
+        return st(*out[0:3]), st(*out[3:6]), st(*out[6:9])
+
+    def write_component(self, comp, arr):
+        arr = np.asarray(arr, dtype=np.float64)
+        if comp == COMP_MASS:
+            a = np.ascontiguousarray(arr)
+            self._check(self.lib.phys_component_write(self.h, comp, _p(a), None, None),
+                        "phys_component_write")
+        else:
+            A = [_col(arr, k) for k in range(3)]
+            self._check(self.lib.phys_component_write(self.h, comp, *[_p(a) for a in A]),
+                        "phys_component_write")
+
+    def read_component(self, comp):
+        if comp == COMP_MASS:
+            a = np.empty(self.n)
+            self._check(self.lib.phys_component_read(self.h, comp, _p(a), None, None),
+                        "phys_component_read")
+            return a
+        out = [np.empty(self.n) for _ in range(3)]
+        self._check(self.lib.phys_component_read(self.h, comp, *[_p(a) for a in out]),
+                    "phys_component_read")
+        return np.stack(out, axis=1)
+
+    # ---- gravity ----
+    def gravity_forces(self, params, force=None):
+        """Force += gravity (returns the updated (n,3) array)."""
+        n = self.n
+        f = np.zeros((n, 3)) if force is None else np.asarray(force, np.float64)
+        F = [np.ascontiguousarray(f[:, k]) for k in range(3)]
+        self._check(self.lib.phys_gravity_forces(self.h, ctypes.byref(params),
+                                                 *[_p(a) for a in F]), "phys_gravity_forces")
+        return np.stack(F, axis=1)
+
+    def gravity_accel(self, params, download=True):
+        n = self.n
+        A = [np.empty(n) for _ in range(3)] if download else [None] * 3
+        self._check(self.lib.phys_gravity_accel(self.h, ctypes.byref(params),
+                                                *[_p(a) for a in A]), "phys_gravity_accel")
+        return np.stack(A, axis=1) if download else None
+
+    def verlet_steps(self, params, dt, nsteps):
+        self._check(self.lib.phys_verlet_steps(self.h, ctypes.byref(params), float(dt),
+                                               int(nsteps)), "phys_verlet_steps")
+
+    def verlet_steps_async(self, params, dt, nsteps):
+        self._check(self.lib.phys_verlet_steps_async(self.h, ctypes.byref(params), float(dt),
+                                                     int(nsteps)), "phys_verlet_steps_async")
+
+    def vv_position_step(self, dt):
+        self._check(self.lib.phys_vv_position_step(self.h, float(dt)), "phys_vv_position_step")
+
+    def vv_velocity_step(self, dt):
+        self._check(self.lib.phys_vv_velocity_step(self.h, float(dt)), "phys_vv_velocity_step")
+
+    def diagnostics(self, G):
+        out = np.zeros(5)
+        self._check(self.lib.phys_diagnostics(self.h, float(G), _p(out)), "phys_diagnostics")
+        return out
+
+    def timings(self):
+        t = Timings()
+        self._check(self.lib.phys_last_timings(self.h, ctypes.byref(t)), "phys_last_timings")
+        return t.as_dict()
+
+    def probe_peaks(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.phys_probe_peaks(self.h, ctypes.byref(a), ctypes.byref(b)),
+                    "phys_probe_peaks")
+        return a.value, b.value
+
+    def bh_export(self, params):
+        n = self.n
+        cap = 4 * n + 64
+        nn = ctypes.c_int64()
+        depth = np.zeros(cap, np.int32)
+        count = np.zeros(cap, np.int64)
+        mass = np.zeros(cap)
+        com = np.zeros(3 * cap)
+        leaf_body = np.zeros(cap, np.int64)
+        body_leaf = np.zeros(n, np.int64)
+        khi = np.zeros(n, np.uint64)
+        klo = np.zeros(n, np.uint64)
+        perm = np.zeros(n, np.int64)
+        root4 = np.zeros(4)
+        self._check(self.lib.phys_bh_export(
+            self.h, ctypes.byref(params), cap, ctypes.byref(nn), _p(depth, _I32), _p(count, _I64),
+            _p(mass), _p(com), _p(leaf_body, _I64), _p(body_leaf, _I64), _p(khi, _U64),
+            _p(klo, _U64), _p(perm, _I64), _p(root4)), "phys_bh_export")
+        k = nn.value
+        assert k <= cap
+        return dict(depth=depth[:k], count=count[:k], mass=mass[:k],
+                    com=com[:3 * k].reshape(k, 3), leaf_body=leaf_body[:k], body_leaf=body_leaf,
+                    keys_hi=khi, keys_lo=klo, perm=perm, root=root4, nnodes=k)
+
+
+# ---------------------------------------------------------------------------
+# Mirror of the reference's gravity plugin API (bevy_ecs systems).
+# ---------------------------------------------------------------------------
+G_SI = 6.67430e-11  # src/core/constants.rs:7
+
+
+@dataclass
+class UniverseConfig:
+    """src/core/config.rs:26-79 (fields on the gravity path, same defaults)."""
+    gravitational_constant: float = G_SI
+    softening_epsilon: float = 1e-4
+    barnes_hut_theta: float = 0.5
+    sector_size: float = 1e12
+
+
+@dataclass
+class SimulationTime:
+    """src/core/time.rs:16-77 (the fixed dt the integrators read)."""
+    dt: float = 1.0 / 60.0
+    tick: int = 0
+    elapsed: float = 0.0
+
+    @staticmethod
+    def with_dt(dt):
+        return SimulationTime(dt=dt)
+
+    def advance_tick(self):
+        self.tick += 1
+        self.elapsed += self.dt
+
+
+@dataclass
+class World:
+    """Structure-of-arrays body store holding the components the gravity path
+    reads and writes (Force, Mass, Sector, LocalPosition, Velocity,
+    Acceleration, PreviousAcceleration; src/components/dynamics.rs:13-37,
+    src/core/coordinates.rs:19-26).  Row order is the query order."""
+    mass: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    local: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    sector: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int64))
+    velocity: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    force: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    acceleration: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    prev_acceleration: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+
+    def spawn(self, mass, local, sector=(0, 0, 0), velocity=(0.0, 0.0, 0.0),
+              acceleration=(0.0, 0.0, 0.0), prev_acceleration=(0.0, 0.0, 0.0)):
+        """Add one body; returns its row (the 'entity')."""
+        self.mass = np.append(self.mass, float(mass))
+        self.local = np.vstack([self.local, np.asarray(local, np.float64)[None]])
+        self.sector = np.vstack([self.sector, np.asarray(sector, np.int64)[None]])
+        self.velocity = np.vstack([self.velocity, np.asarray(velocity, np.float64)[None]])
+        self.force = np.vstack([self.force, np.zeros((1, 3))])
+        self.acceleration = np.vstack([self.acceleration, np.asarray(acceleration, np.float64)[None]])
+        self.prev_acceleration = np.vstack(
+            [self.prev_acceleration, np.asarray(prev_acceleration, np.float64)[None]])
+        return self.mass.shape[0] - 1
+
+    @staticmethod
+    def from_arrays(pos, vel, m):
+        n = len(m)
+        return World(mass=np.asarray(m, np.float64).copy(), local=np.asarray(pos, np.float64).copy(),
+                     sector=np.zeros((n, 3), np.int64),
+                     velocity=np.zeros((n, 3)) if vel is None else np.asarray(vel, np.float64).copy(),
+                     force=np.zeros((n, 3)), acceleration=np.zeros((n, 3)),
+                     prev_acceleration=np.zeros((n, 3)))
+
+    def __len__(self):
+        return int(self.mass.shape[0])
+
+
+_default_ctx = None
+
+
+def default_context():
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def _gravity_system(world, config, method, precision, leaf_cap, ctx, bh_quirk):
+    ctx = ctx or default_context()
+    if len(world) < 2:  # gravity.rs:49-51
+        return
+    ctx.upload_sectors(world.sector, world.local, config.sector_size, world.mass,
+                       bh_quirk=bh_quirk)
+    p = make_params(config.gravitational_constant, config.softening_epsilon,
+                    config.barnes_hut_theta, method, precision, leaf_cap)
+    world.force = ctx.gravity_forces(p, world.force)
+
+
+def brute_force_gravity_system(world, config, precision=F64_EXACT, ctx=None):
+    """src/physics/gravity.rs:27-74 on the GPU: Force += softened direct sum."""
+    _gravity_system(world, config, DIRECT, precision, 1, ctx, bh_quirk=False)
+
+
+def barnes_hut_gravity_system(world, config, precision=F64_EXACT, leaf_cap=1, ctx=None):
+    """src/physics/gravity_tree.rs:260-338 on the GPU: Force += Barnes-Hut."""
+    _gravity_system(world, config, BARNES_HUT, precision, leaf_cap, ctx, bh_quirk=True)
+
+
+def reset_forces(world):
+    """src/physics/forces.rs:15-19."""
+    world.force[:] = 0.0
+
+
+def _state_to_ctx(world, ctx, config=None):
+    ctx.upload_sectors(world.sector, world.local,
+                       config.sector_size if config else 1e12, world.mass,
+                       vel=world.velocity)
+    ctx.write_component(COMP_ACCELERATION, world.acceleration)
+    ctx.write_component(COMP_PREV_ACCELERATION, world.prev_acceleration)
+
+
+def compute_acceleration_system(world, ctx=None):
+    """src/physics/integrators.rs:110-118: a = F / m (IEEE division)."""
+    world.acceleration = world.force / world.mass[:, None]
+
+
+def velocity_verlet_position_system(world, time, ctx=None):
+    """src/physics/integrators.rs:63-83 on the device."""
+    ctx = ctx or default_context()
+    _state_to_ctx(world, ctx)
+    ctx.vv_position_step(time.dt)
+    world.local = ctx.read_component(COMP_POSITION)
+    world.prev_acceleration = ctx.read_component(COMP_PREV_ACCELERATION)
+
+
+def velocity_verlet_velocity_system(world, time, ctx=None):
+    """src/physics/integrators.rs:92-104 on the device."""
+    ctx = ctx or default_context()
+    _state_to_ctx(world, ctx)
+    ctx.vv_velocity_step(time.dt)
+    world.velocity = ctx.read_component(COMP_VELOCITY)
+
+
+def energy_diagnostics(world, config, ctx=None):
+    """src/physics/energy.rs:21-56 + integrators.rs:123-129 on the device:
+    returns (kinetic, potential, momentum (3,))."""
+    ctx = ctx or default_context()
+    ctx.upload_sectors(world.sector, world.local, config.sector_size, world.mass,
+                       vel=world.velocity)
+    out = ctx.diagnostics(config.gravitational_constant)
+    return out[0], out[1], out[2:5]
