@@ -1,0 +1,376 @@
+"""Benchmark: particle-steps/s of Velocity-Verlet steps with Barnes-Hut gravity.
+
+Workload (default): N = 2^20 equal-mass Plummer sphere (a = 1, G = 1, seed =
+rank), theta = 0.5, eps = 0.01, dt = 1e-3, leaf capacity 8, FP32-compensated
+pair terms with FP64 state.  One step = one Velocity-Verlet tick on the device:
+bounding cube, descent keys, radix sort, octree + centre of mass, theta walk,
+kick/drift.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun, one rank per GPU): every rank integrates its own
+independent system (replicas, weak scaling; the path has no exchange step);
+time is the max over ranks.  `--impl reference` times the reference's CPU
+algorithm (the C++ oracle restatement: serial pointer-octree build + threaded
+walk, two force evaluations per tick as the reference schedule runs them) on
+the host cores, rank 0 only.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for _p in (REPO, os.path.join(REPO, "phys-rs_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = ("particle-steps/s, 1M-body BH θ=0.5: FP32-comp vs FP64 GPU at ≤1e-6 accel error")
+FLOPS_PER_INTERACTION = 20  # Nyland, Harris & Prins (GPU Gems 3, ch. 31)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--leaf-cap", type=int, default=8)
+    ap.add_argument("--theta", type=float, default=0.5)
+    ap.add_argument("--eps", type=float, default=0.01)
+    ap.add_argument("--dt", type=float, default=1e-3)
+    ap.add_argument("--no-extras", action="store_true", help="skip FP64 comparison and accuracy")
+    ap.add_argument("--quick", action="store_true",
+                    help="device-resident timing only (no e2e, extras, CPU baseline): profiling")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_tick(pos, vel, m, args, sample, rng, nthreads):
+    """One reference Velocity-Verlet tick at full N on the host, with the
+    walk timed on `sample` random targets and scaled to N (two force
+    evaluations per tick, src/main.rs:109,128).  Returns seconds per tick and
+    the parts."""
+    import oracle
+    n = len(m)
+    targets = np.sort(rng.choice(n, size=min(sample, n), replace=False))
+    t0 = time.perf_counter()
+    _, tm = oracle.bh_forces_targets(pos, m, 1.0, args.eps, args.theta, targets,
+                                     nthreads=nthreads)
+    wall = time.perf_counter() - t0
+    build_s, walk_s = tm[0], tm[1] * n / len(targets)
+    # integrator systems: O(N) f64 updates, measured on the same arrays
+    t1 = time.perf_counter()
+    x = pos + vel * args.dt
+    _ = vel + x * 0.5 * args.dt
+    vv_s = time.perf_counter() - t1
+    eval_s = build_s + walk_s
+    return 2.0 * eval_s + vv_s, {"build_s": build_s, "walk_s_scaled": walk_s, "vv_s": vv_s,
+                                 "sample_targets": len(targets), "wall_s": wall}
+
+
+def run_reference(args, ws, rank):
+    import oracle
+    oracle.lib()
+    if rank != 0:
+        return 0
+    import physgpu.ics as ics
+    pos, vel, m = ics.plummer(args.n, seed=0)
+    nthreads = oracle.ncpu()
+    rng = np.random.default_rng(1)
+    sample = 16384
+    for _ in range(args.warmup):
+        cpu_reference_tick(pos, vel, m, args, sample, rng, nthreads)
+    ticks, parts = [], None
+    for _ in range(args.steps):
+        t, parts = cpu_reference_tick(pos, vel, m, args, sample, rng, nthreads)
+        ticks.append(t)
+    t_tick = sum(ticks) / len(ticks)
+    value = args.n / t_tick
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_tick * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Plummer)",
+        "config": workload_config(args, precision="f64", leaf_cap=1),
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": nthreads,
+                         "kind": "port",
+                         "sample": ("per tick: serial pointer-octree build of all %d bodies + "
+                                    "threaded walk of %d random targets scaled to N, x2 force "
+                                    "evaluations per tick; last tick %s" % (
+                                        args.n, parts["sample_targets"],
+                                        json.dumps({k: round(v, 4) for k, v in parts.items()})))},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(args, precision, leaf_cap):
+    return {"workload": "barnes_hut_plummer_n%d" % args.n, "n": args.n, "theta": args.theta,
+            "eps": args.eps, "G": 1.0, "dt": args.dt, "leaf_cap": leaf_cap,
+            "precision": precision, "ics": "Plummer a=1, equal masses 1/N, seed=rank",
+            "l2": "flushed between timed steps (256 MiB write)"}
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+
+    import physgpu
+    import physgpu.ics as ics
+    from physgpu import BARNES_HUT, F32C, F64, make_params
+
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local))
+    ctx = physgpu.Context(local)
+    lib = ctx.lib
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    pos, vel, m = ics.plummer(args.n, seed=rank)
+    n = args.n
+    p32 = make_params(1.0, args.eps, args.theta, BARNES_HUT, F32C, args.leaf_cap)
+    p64 = make_params(1.0, args.eps, args.theta, BARNES_HUT, F64, args.leaf_cap)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def timed_steps(params, k, flush=True):
+        """k ticks, each bracketed by CUDA events on the library's stream,
+        L2 flushed between ticks; returns (total_ms, walk_ms_list, interactions)."""
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(k)]
+        walk, inter = [], []
+        with torch.cuda.stream(stream):
+            for i in range(k):
+                if flush:
+                    flush_buf.fill_(i & 0xff)
+                evs[i][0].record(stream)
+                ctx.verlet_steps(params, args.dt, 1)
+                evs[i][1].record(stream)
+                t = ctx.timings()
+                walk.append(t["walk_ms"])
+                inter.append(t["interactions"])
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in evs), walk, inter
+
+    # ---- device-resident value: F32C ----
+    ctx.upload(pos, vel, m)
+    for _ in range(args.warmup):
+        ctx.verlet_steps(p32, args.dt, 1)
+    launches0 = ctx.timings()["launches"]
+    clocks = Clocks(local)
+    clocks.start()
+    barrier()
+    tot_ms, walk_ms, inter = timed_steps(p32, args.steps)
+    barrier()
+    clk = clocks.stop()
+    launches = ctx.timings()["launches"] - launches0
+    t_all = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        torch.distributed.all_reduce(t_all, op=torch.distributed.ReduceOp.MAX)
+    t_max_ms = float(t_all.item())
+    value = ws * n * args.steps / (t_max_ms * 1e-3)
+    tm = ctx.timings()
+
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"quick": True, "value": value, "ms_per_step": t_max_ms / args.steps,
+                              "walk_ms": statistics.median(walk_ms),
+                              "interactions": statistics.median(inter),
+                              "timings": ctx.timings()}), flush=True)
+        ctx.close()
+        return 0
+
+    # ---- e2e through the C ABI with pinned host buffers ----
+    def pinned(k):
+        return torch.empty(k, dtype=torch.float64, pin_memory=True)
+
+    X = [pinned(n) for _ in range(3)]
+    V = [pinned(n) for _ in range(3)]
+    A = [pinned(n) for _ in range(3)]
+    M = pinned(n)
+    for k in range(3):
+        X[k].copy_(torch.from_numpy(np.ascontiguousarray(pos[:, k])))
+        V[k].copy_(torch.from_numpy(np.ascontiguousarray(vel[:, k])))
+    M.copy_(torch.from_numpy(m))
+    ctx.upload(pos, vel, m)
+    ctx.gravity_accel(p32, download=False)
+    ptr = lambda t: ctypes.cast(t.data_ptr(), ctypes.POINTER(ctypes.c_double))
+    lib.phys_state_download(ctx.h, None, None, None, None, None, None, *[ptr(a) for a in A])
+    h2d = n * 8 * 10
+    d2h = n * 8 * 9
+
+    def e2e_step():
+        st = lib.phys_state_upload(ctx.h, n, *[ptr(a) for a in X], *[ptr(a) for a in V], ptr(M))
+        st = st or lib.phys_state_set_accel(ctx.h, *[ptr(a) for a in A])
+        st = st or lib.phys_verlet_steps(ctx.h, ctypes.byref(p32), args.dt, 1)
+        st = st or lib.phys_state_download(ctx.h, *[ptr(a) for a in X], *[ptr(a) for a in V],
+                                           *[ptr(a) for a in A])
+        if st:
+            raise physgpu.PhysError(st, lib.phys_last_error(ctx.h).decode())
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = ws * n * args.steps / (float(e2e_t.item()) * 1e-3)
+
+    extras = {}
+    if not args.no_extras:
+        # ---- FP64 form of the same step (same tree, same workload) ----
+        ctx.upload(pos, vel, m)
+        for _ in range(args.warmup):
+            ctx.verlet_steps(p64, args.dt, 1)
+        barrier()
+        t64, walk64, _ = timed_steps(p64, args.steps)
+        extras["fp64_ms_per_step"] = t64 / args.steps
+        extras["fp64_walk_ms"] = statistics.median(walk64)
+        extras["speedup_f32c_vs_fp64_step"] = t64 / tot_ms
+        # ---- accuracy: F32C vs F64 on the same tree, initial positions ----
+        ctx.upload(pos, vel, m)
+        a64 = ctx.gravity_accel(p64)
+        a32 = ctx.gravity_accel(p32)
+        e = np.linalg.norm(a32 - a64, axis=1) / np.linalg.norm(a64, axis=1)
+        extras["accel_err_f32c_vs_fp64_same_tree"] = {
+            "median": float(np.median(e)), "p99": float(np.quantile(e, 0.99)),
+            "max": float(e.max())}
+        pcap1 = make_params(1.0, args.eps, args.theta, BARNES_HUT, F32C, 1)
+        ctx.upload(pos, vel, m)
+        for _ in range(2):
+            ctx.verlet_steps(pcap1, args.dt, 1)
+        c1, _, _ = timed_steps(pcap1, max(2, args.steps // 2))
+        extras["leaf_cap1_ms_per_step"] = c1 / max(2, args.steps // 2)
+
+    # ---- roofline of the dominant kernel (the walk) ----
+    fp32_tf, fp64_tf = ctx.probe_peaks()
+    walk_med = statistics.median(walk_ms)
+    inter_med = statistics.median(inter)
+    achieved = FLOPS_PER_INTERACTION * inter_med / (walk_med * 1e-3) / 1e12
+    roof = {"kernel": "walk_kernel<f32c>", "bound": "fp32", "achieved": achieved,
+            "peak": fp32_tf, "unit": "TFLOP/s", "frac": achieved / fp32_tf,
+            "peak_source": "measured live: FFMA loop on all SMs (FMA = 2 flops)",
+            "flops_per_interaction": FLOPS_PER_INTERACTION,
+            "interactions_per_launch": inter_med, "walk_ms": walk_med,
+            "traffic": None, "fp64_peak_tflops": fp64_tf,
+            "phase_ms_last_step": {k: round(tm[k], 4) for k in
+                                   ("bbox_ms", "keys_ms", "sort_ms", "tree_ms", "walk_ms")}}
+
+    # ---- CPU baseline (rank 0, N=1): reference algorithm on a bounded sample ----
+    cpu = None
+    if rank == 0 and ws == 1:
+        import oracle
+        oracle.lib()
+        nth = oracle.ncpu()
+        t_tick, parts = cpu_reference_tick(pos, vel, m, args, 16384, np.random.default_rng(1), nth)
+        cpu = {"value": n / t_tick, "unit": "particle-steps/s", "cores": nth, "kind": "port",
+               "sample": ("one reference tick at N=%d: serial pointer-octree build + threaded "
+                          "walk of %d targets scaled to N, x2 evaluations per tick; parts %s" % (
+                              n, parts["sample_targets"],
+                              json.dumps({k: round(v, 4) for k, v in parts.items()})))}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32c",
+            "data": "synthetic (seeded Plummer sphere; no dataset)",
+            "config": workload_config(args, "f32c (f32 pair terms, two-sum, f64 state)",
+                                      args.leaf_cap),
+            "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches, "clocks": clk, "roofline": roof, "cpu_baseline": cpu,
+            "interactions_per_step": inter_med, "nodes": tm["nodes"], "tree_depth_max": tm["max_depth"],
+        }
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank)
+    return run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

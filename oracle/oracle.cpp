@@ -27,6 +27,7 @@
 #include <cstdint>
 #include <cstring>
 #include <thread>
+#include <utility>
 #include <vector>
 
 namespace {
@@ -233,7 +234,8 @@ struct Exporter {
   int64_t* count;
   double *mass, *cx, *cy, *cz;
   int64_t* leaf_body;  // -1 for internal nodes
-  int64_t* body_leaf;  // per body: pre-order id of the leaf that stores it
+  int64_t* body_leaf;  // per body: pre-order id of the leaf whose cell holds it
+  std::vector<std::pair<const Node*, int64_t>> ids;
   void visit(const Node& nd) {
     if (nd.kind == kEmpty) return;
     int64_t id = cnt++;
@@ -245,8 +247,8 @@ struct Exporter {
       cy[id] = nd.com.y;
       cz[id] = nd.com.z;
       leaf_body[id] = nd.kind == kLeaf ? nd.body.index : -1;
-      if (nd.kind == kLeaf && body_leaf) body_leaf[nd.body.index] = id;
     }
+    ids.emplace_back(&nd, id);
     if (nd.kind == kInternal)
       for (int c = 0; c < 8; ++c) visit(nd.children[c]);
   }
@@ -386,8 +388,20 @@ int64_t oracle_bh_export(int64_t n, const double* x, const double* y, const doub
   }
   if (body_leaf)
     for (int64_t i = 0; i < n; ++i) body_leaf[i] = -1;
-  Exporter E{cap, 0, depth, count, mass, cx, cy, cz, leaf_body, body_leaf};
+  Exporter E{cap, 0, depth, count, mass, cx, cy, cz, leaf_body, body_leaf, {}};
   E.visit(T.root);
+  if (body_leaf) {
+    // Cell membership: follow the insertion rule (octant per level) down to
+    // the leaf whose cell holds each body; guard leaves hold every body that
+    // reached them, including the ones whose slot was overwritten.
+    std::sort(E.ids.begin(), E.ids.end());
+    for (int64_t i = 0; i < n; ++i) {
+      const Node* nd = &T.root;
+      while (nd->kind == kInternal) nd = &nd->children[nd->octant(T.bodies[i].pos)];
+      auto it = std::lower_bound(E.ids.begin(), E.ids.end(), std::make_pair(nd, int64_t(-1)));
+      body_leaf[i] = (it != E.ids.end() && it->first == nd) ? it->second : -1;
+    }
+  }
   return E.cnt;
 }
 

@@ -209,11 +209,13 @@ int verlet_steps(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, b
   if (!(dt == dt)) return fail(c, PHYS_ERR_ARG, "dt is NaN");
   PHYS_TRY(reset_status(c));
   PHYS_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
-  if (!c->accel_valid || !same_params(c->accel_params, *p)) {
+  // accel_params.method == -1: the caller supplied a(x) (Acceleration
+  // component), valid whatever the params.
+  if (!c->accel_valid || (c->accel_params.method != -1 && !same_params(c->accel_params, *p))) {
     PHYS_TRY(eval(c, p, false));  // chain 1 force pass of the first tick
     c->accel_valid = true;
-    c->accel_params = *p;
   }
+  c->accel_params = *p;
   for (int64_t s = 0; s < nsteps; ++s) {
     if (s == 0) PHYS_TRY(verlet_drift(c, dt));
     c->accel_valid = false;
