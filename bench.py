@@ -308,6 +308,17 @@ def run_ours(args, ws, rank, local):
         extras["accel_err_f32c_vs_fp64_same_tree"] = {
             "median": float(np.median(e)), "p99": float(np.quantile(e, 0.99)),
             "max": float(e.max())}
+        # ---- BH truncation vs the f64 direct sum on a 65,536-body subsample ----
+        sub = np.sort(np.random.default_rng(7).choice(n, size=min(65536, n), replace=False))
+        pd = make_params(1.0, args.eps, args.theta, physgpu.DIRECT, F64, 1)
+        t0 = time.perf_counter()
+        ad = ctx.direct_accel_targets(pd, sub)
+        extras["direct_f64_subsample_s"] = time.perf_counter() - t0
+        for name, a in (("f32c_bh", a32), ("f64_bh", a64)):
+            e = np.linalg.norm(a[sub] - ad, axis=1) / np.linalg.norm(ad, axis=1)
+            extras["accel_err_%s_vs_f64_direct_subsample" % name] = {
+                "median": float(np.median(e)), "p99": float(np.quantile(e, 0.99)),
+                "max": float(e.max()), "targets": int(len(sub))}
         pcap1 = make_params(1.0, args.eps, args.theta, BARNES_HUT, F32C, 1)
         ctx.upload(pos, vel, m)
         for _ in range(2):

@@ -144,6 +144,13 @@ int phys_gravity_forces(phys_ctx* ctx, const phys_params* p, double* fx, double*
  * and caches a(x) for phys_verlet_steps. */
 int phys_gravity_accel(phys_ctx* ctx, const phys_params* p, double* ax, double* ay, double* az);
 
+/* Direct-sum accelerations (a = F/m, all n sources) for a subset of targets:
+ * targets[k] in [0, n), results in ax[k] (host arrays of length nt).  Used as
+ * the f64 direct-sum reference for Barnes-Hut runs at sizes where the full
+ * O(N^2) sum is too costly.  p->method is ignored (direct sum). */
+int phys_direct_accel_targets(phys_ctx* ctx, const phys_params* p, int64_t nt,
+                              const int64_t* targets, double* ax, double* ay, double* az);
+
 /* ---- integration -------------------------------------------------------- */
 /* nsteps Velocity-Verlet ticks on the device-resident state: each tick is
  * velocity_verlet_position_system (integrators.rs:63-83), a force evaluation

@@ -25,14 +25,34 @@ constexpr int kMetaGuard = 1 << 9;   // leaf at the guard depth D* (gravity_tree
 constexpr int kMetaGate = 1 << 10;   // total_mass > 0 (children are visited only then,
                                      // gravity_tree.rs:201)
 
+// Walk records (array of structures, 48 B, one per node, read with three
+// independent 16-B loads):
+//   l = {next, self, start, meta}: self = sorted position of the body a
+//   one-body leaf stores (-1 otherwise, also the self-exclusion test);
+//   start = first body of a bucket leaf; meta = depth | kWLeaf | count << 8.
+//   A cell whose total mass is not > 0 (other than the root) gets depth
+//   kWSkip, which no lane can be active at, so the warp jumps over it.
+constexpr int kWDepth = 63;
+constexpr int kWSkip = 63;
+constexpr int kWLeaf = 1 << 6;
+struct __align__(16) Rec32 {
+  float4 a;  // x_hi, y_hi, z_hi, mass
+  float4 b;  // x_lo, y_lo, z_lo, ropen2 = s_d^2 / theta^2 (-1: one-body leaf, always taken)
+  int4 l;
+};
+struct __align__(16) Rec64 {
+  double4 a;  // x, y, z, mass
+  int4 l;
+};
+
 struct BhTree {
   int64_t n = 0;
   int64_t nnodes = 0;
   int leaf_cap = 1;
   const int4* link = nullptr;
-  const double4* rec64 = nullptr;
-  const float4* rec_hi = nullptr;
-  const float4* rec_lo = nullptr;
+  const double4* rec64 = nullptr;     // exact walk: record per node (with `link`)
+  const Rec32* w32 = nullptr;         // F32C walk records
+  const Rec64* w64 = nullptr;         // F64 walk records
   const double4* mc = nullptr;
   const uint32_t* perm = nullptr;     // sorted position -> caller index
   const double4* body64 = nullptr;    // sorted bodies (x, y, z, m)

@@ -107,6 +107,8 @@ enum WsSlot {
 // direct.cu
 int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, double* oy,
                 double* oz);
+int direct_targets(phys_ctx* c, const phys_params* p, int64_t nt, const int64_t* d_tidx,
+                   double* ox, double* oy, double* oz);
 // tree.cu
 int bh_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, double* oy,
             double* oz);

@@ -531,6 +531,35 @@ int phys_gravity_accel(phys_ctx* c, const phys_params* p, double* ax, double* ay
   return st;
 }
 
+int phys_direct_accel_targets(phys_ctx* c, const phys_params* p, int64_t nt,
+                              const int64_t* targets, double* ax, double* ay, double* az) {
+  if (!c) return PHYS_ERR_ARG;
+  PHYS_TRY(check_params(c, p));
+  if (nt < 0 || (nt > 0 && (!targets || !ax || !ay || !az)))
+    return fail(c, PHYS_ERR_ARG, "targets and outputs are required");
+  if (c->n < 2 || nt == 0) {
+    for (int64_t k = 0; k < nt; ++k) ax[k] = ay[k] = az[k] = 0.0;
+    return PHYS_OK;
+  }
+  int st = PHYS_OK;
+  int64_t* dt = (int64_t*)ws_get(c, WS_ADJ3, sizeof(int64_t) * nt, &st);
+  if (st) return st;
+  double* out = (double*)ws_get(c, WS_ADJ2, sizeof(double) * 3 * nt, &st);
+  if (st) return st;
+  PHYS_TRY(reset_status(c));
+  PHYS_CUDA(c, cudaMemcpyAsync(dt, targets, sizeof(int64_t) * nt, cudaMemcpyHostToDevice, c->stream));
+  PHYS_TRY(direct_targets(c, p, nt, dt, out, out + nt, out + 2 * nt));
+  PHYS_TRY(d2h(c, ax, out, nt));
+  PHYS_TRY(d2h(c, ay, out + nt, nt));
+  PHYS_TRY(d2h(c, az, out + 2 * nt, nt));
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  int32_t sw = 0;
+  PHYS_TRY(read_status(c, &sw));
+  if (sw & kStatOverflow) return fail(c, PHYS_ERR_ARG, "target index out of range");
+  if (sw & kStatNonfinite) return fail(c, PHYS_ERR_NONFINITE, "non-finite result");
+  return PHYS_OK;
+}
+
 int phys_verlet_steps(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps) {
   if (!c) return PHYS_ERR_ARG;
   return verlet_steps(c, p, dt, nsteps, true);

@@ -275,6 +275,73 @@ __global__ void slice_reduce_kernel(int64_t n, int nslices, const double* __rest
   }
 }
 
+// Subset of targets (index list), all sources; one thread per (target,
+// slice).  The self pair is skipped by index.  F64_EXACT keeps the reference
+// op order with one slice; F64 / F32C use FMA + rsqrt in f64 (the subset
+// serves as the f64 reference, so F32C is not used here).
+__global__ void __launch_bounds__(kTile)
+direct_targets_kernel(int64_t n, int64_t nt, const int64_t* __restrict__ tidx, int64_t slice_len,
+                      const double* __restrict__ x, const double* __restrict__ y,
+                      const double* __restrict__ z, const double* __restrict__ m, double G,
+                      double eps2, int exact, double* __restrict__ part, double* __restrict__ ox,
+                      double* __restrict__ oy, double* __restrict__ oz, int32_t* status) {
+  __shared__ double4 tile[kTile];
+  const int64_t t = blockIdx.x * (int64_t)kTile + threadIdx.x;
+  const bool valid = t < nt;
+  const int64_t i = valid ? tidx[t] : -1;
+  const bool ok = valid && i >= 0 && i < n;
+  if (valid && !ok) atomicOr(status, kStatOverflow);
+  const double xi = ok ? x[i] : 0.0, yi = ok ? y[i] : 0.0, zi = ok ? z[i] : 0.0;
+  const double mi = ok ? m[i] : 0.0;
+  const double gm = xmul(G, mi);
+  const int64_t lo = blockIdx.y * slice_len;
+  const int64_t hi = min64(n, lo + slice_len);
+  double ax = 0.0, ay = 0.0, az = 0.0;
+  for (int64_t base = lo; base < hi; base += kTile) {
+    const int64_t j = base + threadIdx.x;
+    __syncthreads();
+    tile[threadIdx.x] = j < hi ? make_double4(x[j], y[j], z[j], m[j]) : make_double4(0, 0, 0, 0);
+    __syncthreads();
+    const int cnt = (int)min64(kTile, hi - base);
+    if (exact) {
+      for (int k = 0; k < cnt; ++k) {
+        if (base + k == i) continue;
+        const double4 s = tile[k];
+        const double rx = xsub(s.x, xi), ry = xsub(s.y, yi), rz = xsub(s.z, zi);
+        const double s2 = xadd(xlen2(rx, ry, rz), eps2);
+        const double sc = xdiv(xmul(gm, s.w), xmul(s2, xsqrt(s2)));
+        ax = xadd(ax, xmul(rx, sc));
+        ay = xadd(ay, xmul(ry, sc));
+        az = xadd(az, xmul(rz, sc));
+      }
+    } else {
+#pragma unroll 4
+      for (int k = 0; k < cnt; ++k) {
+        const double4 s = tile[k];
+        const double rx = s.x - xi, ry = s.y - yi, rz = s.z - zi;
+        const bool self = base + k == i;
+        const double r2 = self ? 1.0 : fma(rx, rx, fma(ry, ry, fma(rz, rz, eps2)));
+        const double inv = rsqrt(r2);
+        const double w = self ? 0.0 : s.w * (inv * inv * inv);
+        ax = fma(rx, w, ax);
+        ay = fma(ry, w, ay);
+        az = fma(rz, w, az);
+      }
+    }
+  }
+  if (!valid) return;
+  if (exact) {  // a = F / m
+    ox[t] = xdiv(ax, mi);
+    oy[t] = xdiv(ay, mi);
+    oz[t] = xdiv(az, mi);
+    return;
+  }
+  double* pp = part + (size_t)blockIdx.y * 3 * nt;
+  pp[t] = ax;
+  pp[nt + t] = ay;
+  pp[2 * nt + t] = az;
+}
+
 // Slices so that about two waves of 148 SMs x 2048 threads are resident;
 // every slice spans whole tiles.
 int64_t choose_slices(int64_t n) {
@@ -333,6 +400,33 @@ int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, 
   c->tm.bbox_ms = c->tm.keys_ms = c->tm.sort_ms = c->tm.tree_ms = 0.0;
   c->tm.nodes = 0;
   c->tm.max_depth = 0;
+  return PHYS_OK;
+}
+
+int direct_targets(phys_ctx* c, const phys_params* p, int64_t nt, const int64_t* d_tidx,
+                   double* ox, double* oy, double* oz) {
+  const int64_t n = c->n;
+  const double eps2 = p->eps * p->eps;
+  const bool exact = p->precision == PHYS_F64_EXACT;
+  int64_t nsl = 1;
+  if (!exact) {
+    nsl = ceil_div(148LL * 2048, ceil_div(nt, kTile) * kTile);
+    if (nsl > ceil_div(n, kTile)) nsl = ceil_div(n, kTile);
+    if (nsl < 1) nsl = 1;
+  }
+  const int64_t slice_len = ceil_div(ceil_div(n, nsl), kTile) * kTile;
+  nsl = ceil_div(n, slice_len);
+  int st = PHYS_OK;
+  double* part = (double*)ws_get(c, WS_DIRECT_PART, sizeof(double) * 3 * nt * nsl, &st);
+  if (st) return st;
+  dim3 grid((unsigned)ceil_div(nt, kTile), (unsigned)nsl);
+  PHYS_LAUNCH(c, direct_targets_kernel, grid, kTile, 0, n, nt, d_tidx, slice_len, c->x, c->y,
+              c->z, c->m, p->G, eps2, (int)exact, part, ox, oy, oz, c->d_status);
+  if (!exact) {
+    int g = (int)min64(ceil_div(nt, 256), 148 * 8);
+    PHYS_LAUNCH(c, slice_reduce_kernel, g, 256, 0, nt, (int)nsl, part, c->m, p->G, 0, ox, oy, oz,
+                c->d_status);
+  }
   return PHYS_OK;
 }
 

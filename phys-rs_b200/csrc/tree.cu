@@ -518,8 +518,8 @@ com_recurrence_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
 // into com = S/M here) or finished (com, M) (reference form).
 __global__ void __launch_bounds__(kBlock)
 finalize_kernel(int64_t nnodes, int4* __restrict__ link, double4* __restrict__ mc, int sums,
-                int leaf_cap, const double4* __restrict__ body64, double4* __restrict__ rec64,
-                float4* __restrict__ rec_hi, float4* __restrict__ rec_lo) {
+                int leaf_cap, const double4* __restrict__ body64, const TreeHeader* __restrict__ hdr,
+                double4* __restrict__ rec64, Rec32* __restrict__ w32, Rec64* __restrict__ w64) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnodes;
        k += (int64_t)gridDim.x * blockDim.x) {
     int4 lk = link[k];
@@ -532,26 +532,40 @@ finalize_kernel(int64_t nnodes, int4* __restrict__ link, double4* __restrict__ m
         a = make_double4(0.0, 0.0, 0.0, M);
       mc[k] = a;
     }
-    if (a.w > 0.0) lk.w |= kMetaGate;
+    const bool gate = a.w > 0.0;
+    if (gate) lk.w |= kMetaGate;
     link[k].w = lk.w;
+    const int d = lk.w & kMetaDepth;
+    const int cntb = lk.z - lk.y;
+    const bool leaf = lk.w & kMetaLeaf;
+    int self = -1;
     double4 r = a;
-    if (lk.w & kMetaLeaf) {
-      const int cntb = lk.z - lk.y;
-      if (cntb == 1)
-        r = body64[lk.y];
-      else if ((lk.w & kMetaGuard) && leaf_cap == 1)
-        r = body64[lk.z - 1];  // the last inserted (highest index) body
+    if (leaf && cntb == 1) {
+      self = lk.y;
+    } else if (leaf && (lk.w & kMetaGuard) && leaf_cap == 1) {
+      self = lk.z - 1;  // the last inserted (highest index) body
     }
+    if (self >= 0) r = body64[self];
     if (rec64) rec64[k] = r;
-    if (rec_hi) {
-      float4 h, l;
-      split_df(r.x, h.x, l.x);
-      split_df(r.y, h.y, l.y);
-      split_df(r.z, h.z, l.z);
-      h.w = (float)r.w;
-      l.w = 0.f;
-      rec_hi[k] = h;
-      rec_lo[k] = l;
+    int wmeta = (gate || k == 0) ? d : kWSkip;
+    if (leaf && self < 0) wmeta |= kWLeaf | (cntb << 8);
+    const int4 wl = make_int4(lk.x, self, lk.y, wmeta);
+    if (w64) {
+      Rec64 o;
+      o.a = r;
+      o.l = wl;
+      w64[k] = o;
+    }
+    if (w32) {
+      Rec32 o;
+      split_df(r.x, o.a.x, o.b.x);
+      split_df(r.y, o.a.y, o.b.y);
+      split_df(r.z, o.a.z, o.b.z);
+      o.a.w = (float)r.w;
+      // accept iff s^2 < theta^2 d^2  <=>  d^2 > s^2 / theta^2 (inf for theta = 0)
+      o.b.w = self >= 0 ? -1.0f : (float)(hdr->s2[d] / hdr->theta2);
+      o.l = wl;
+      w32[k] = o;
     }
   }
 }
@@ -676,23 +690,23 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t) {
                 arrive, body64, mc, c->d_status);
   }
   double4* rec64 = nullptr;
-  float4 *rec_hi = nullptr, *rec_lo = nullptr;
-  if (!need_f32) {
-    rec64 = WS(double4, WS_NODE_PM, nnodes);
-  } else {
-    rec_hi = WS(float4, WS_NODE_HI, nnodes);
-    rec_lo = WS(float4, WS_NODE_LO, nnodes);
-  }
+  Rec32* w32 = nullptr;
+  Rec64* w64 = nullptr;
+  if (exact) rec64 = WS(double4, WS_NODE_PM, nnodes);
+  if (need_f32)
+    w32 = WS(Rec32, WS_NODE_HI, nnodes);
+  else if (!exact)
+    w64 = WS(Rec64, WS_NODE_LO, nnodes);
   PHYS_LAUNCH(c, finalize_kernel, grid_for(nnodes), kBlock, 0, nnodes, link, mc, exact ? 0 : 1,
-              p->leaf_cap, body64, rec64, rec_hi, rec_lo);
+              p->leaf_cap, body64, c->d_hdr, rec64, w32, w64);
 #undef WS
   t->n = n;
   t->nnodes = nnodes;
   t->leaf_cap = p->leaf_cap;
   t->link = link;
   t->rec64 = rec64;
-  t->rec_hi = rec_hi;
-  t->rec_lo = rec_lo;
+  t->w32 = w32;
+  t->w64 = w64;
   t->mc = mc;
   t->perm = perm;
   t->body64 = body64;

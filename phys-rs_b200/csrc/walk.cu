@@ -37,25 +37,21 @@ __device__ __forceinline__ void warp_count(unsigned ninter, unsigned long long* 
 
 template <bool kF32>
 __global__ void __launch_bounds__(kWalkBlock)
-walk_kernel(int64_t n, int64_t nnodes, const int4* __restrict__ link,
-            const double4* __restrict__ rec64, const float4* __restrict__ rec_hi,
-            const float4* __restrict__ rec_lo, const double4* __restrict__ body64,
-            const float4* __restrict__ body_hi, const float4* __restrict__ body_lo,
-            const uint32_t* __restrict__ perm, const TreeHeader* __restrict__ hdr, double G,
-            double eps2, int want_force, int leaf_cap, double* __restrict__ ox,
-            double* __restrict__ oy, double* __restrict__ oz, unsigned long long* counter,
-            int32_t* status) {
-  __shared__ double s2d[kMaxLevels];
-  __shared__ float s2f[kMaxLevels];
-  for (int d = threadIdx.x; d < kMaxLevels; d += blockDim.x) {
-    s2d[d] = hdr->s2[d];
-    s2f[d] = (float)hdr->s2[d];
+walk_kernel(int n, int nnodes, const Rec32* __restrict__ w32, const Rec64* __restrict__ w64,
+            const double4* __restrict__ body64, const float4* __restrict__ body_hi,
+            const float4* __restrict__ body_lo, const uint32_t* __restrict__ perm,
+            const TreeHeader* __restrict__ hdr, double G, double eps2, int want_force,
+            double* __restrict__ ox, double* __restrict__ oy, double* __restrict__ oz,
+            unsigned long long* counter, int32_t* status) {
+  __shared__ double s2d[kWDepth + 1];
+  if (!kF32) {
+    for (int d = threadIdx.x; d <= kWDepth; d += blockDim.x)
+      s2d[d] = d < kMaxLevels ? hdr->s2[d] : 0.0;
+    __syncthreads();
   }
-  __syncthreads();
   const double theta2 = hdr->theta2;
-  const float theta2f = (float)theta2;
   const float eps2f = (float)eps2;
-  const int64_t p = blockIdx.x * (int64_t)kWalkBlock + threadIdx.x;
+  const int p = blockIdx.x * kWalkBlock + threadIdx.x;
   const bool valid = p < n;
 
   double tx = 0, ty = 0, tz = 0;
@@ -75,30 +71,12 @@ walk_kernel(int64_t n, int64_t nnodes, const int4* __restrict__ link,
   float lx = 0, ly = 0, lz = 0;             //                      (lo)
   float px = 0, py = 0, pz = 0;             // F32C partial since last flush
   unsigned ninter = 0;
-  int open_to = 0;
-  int32_t node = 0;
-  unsigned iter = 0;
+  // open_to = number of consecutive opened levels on the current path; a
+  // lane is active at a node of depth d iff open_to == d.  Lanes past the end
+  // start at -1 and are never active.
+  int open_to = valid ? 0 : -1;
+  int node = 0;
 
-  auto pair64 = [&](double4 s) {
-    const double rx = s.x - tx, ry = s.y - ty, rz = s.z - tz;
-    const double r2 = fma(rx, rx, fma(ry, ry, fma(rz, rz, eps2)));
-    const double inv = rsqrt(r2);
-    const double w = s.w * (inv * inv * inv);
-    ax = fma(rx, w, ax);
-    ay = fma(ry, w, ay);
-    az = fma(rz, w, az);
-  };
-  auto pair32 = [&](float4 h, float4 l) {
-    const float rx = (h.x - thx) + (l.x - tlx);
-    const float ry = (h.y - thy) + (l.y - tly);
-    const float rz = (h.z - thz) + (l.z - tlz);
-    const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2f)));
-    const float inv = rsqrtf(r2);
-    const float w = h.w * (inv * inv * inv);
-    px = fmaf(rx, w, px);
-    py = fmaf(ry, w, py);
-    pz = fmaf(rz, w, pz);
-  };
   auto flush = [&]() {
     float s, e;
     two_sum(hx, px, s, e);
@@ -113,81 +91,101 @@ walk_kernel(int64_t n, int64_t nnodes, const int4* __restrict__ link,
     px = py = pz = 0.f;
   };
 
-  while (node < nnodes) {
-    const int4 lk = link[node];
-    if (lk.x <= node || lk.x > nnodes) {  // malformed tree: report, never spin
-      if ((threadIdx.x & 31) == 0) atomicOr(status, kStatOverflow);
-      break;
-    }
-    const int d = lk.w & kMetaDepth;
-    if (open_to > d) open_to = d;
-    const bool act = valid && open_to == d && ((lk.w & kMetaGate) || node == 0);
-    const int cntb = lk.z - lk.y;
-    const bool leaf = lk.w & kMetaLeaf;
-    if (leaf && (cntb == 1 || ((lk.w & kMetaGuard) && leaf_cap == 1))) {
-      // One stored body: exact pair unless it is the target itself
-      // (gravity_tree.rs:180-187).
-      const int sp = cntb == 1 ? lk.y : lk.z - 1;
-      if (act && sp != p) {
-        if (kF32) pair32(rec_hi[node], rec_lo[node]);
-        else pair64(rec64[node]);
-        ++ninter;
-      }
-      node = lk.x;
+  // Visit body.  Returns the next node; always > node, so the loop ends
+  // even on a malformed tree.
+  auto visit = [&](int nd) -> int {
+    int4 L;
+    float4 A, B;
+    double4 A64;
+    if (kF32) {
+      const Rec32* rp = w32 + nd;
+      A = rp->a;
+      B = rp->b;
+      L = rp->l;
     } else {
-      bool open;
-      if (kF32) {
-        const float4 h = rec_hi[node], l = rec_lo[node];
-        const float rx = (h.x - thx) + (l.x - tlx);
-        const float ry = (h.y - thy) + (l.y - tly);
-        const float rz = (h.z - thz) + (l.z - tlz);
-        const float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-        open = act && !(s2f[d] < theta2f * d2);
-        if (act && !open) {
-          const float r2 = d2 + eps2f;
-          const float inv = rsqrtf(r2);
-          const float w = h.w * (inv * inv * inv);
-          px = fmaf(rx, w, px);
-          py = fmaf(ry, w, py);
-          pz = fmaf(rz, w, pz);
-          ++ninter;
-        }
-      } else {
-        const double4 s = rec64[node];
-        const double rx = s.x - tx, ry = s.y - ty, rz = s.z - tz;
-        const double d2 = fma(rx, rx, fma(ry, ry, rz * rz));
-        open = act && !(s2d[d] < theta2 * d2);
-        if (act && !open) {
-          const double inv = rsqrt(d2 + eps2);
-          const double w = s.w * (inv * inv * inv);
-          ax = fma(rx, w, ax);
-          ay = fma(ry, w, ay);
-          az = fma(rz, w, az);
-          ++ninter;
-        }
+      const Rec64* rp = w64 + nd;
+      A64 = rp->a;
+      L = rp->l;
+    }
+    const int d = L.w & kWDepth;
+    open_to = min(open_to, d);
+    const bool act = open_to == d;
+    bool acc;
+    if (kF32) {
+      const float rx = (A.x - thx) + (B.x - tlx);
+      const float ry = (A.y - thy) + (B.y - tly);
+      const float rz = (A.z - thz) + (B.z - tlz);
+      const float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+      acc = d2 > B.w;  // one-body leaves carry -1: always an exact pair
+      const bool use = act && acc && L.y != p;
+      const float inv = rsqrtf(d2 + eps2f);
+      const float w = use ? A.w * (inv * inv * inv) : 0.f;
+      px = fmaf(rx, w, px);
+      py = fmaf(ry, w, py);
+      pz = fmaf(rz, w, pz);
+      ninter += use;
+    } else {
+      const double rx = A64.x - tx, ry = A64.y - ty, rz = A64.z - tz;
+      const double d2 = fma(rx, rx, fma(ry, ry, rz * rz));
+      acc = L.y >= 0 || s2d[d] < theta2 * d2;  // gravity_tree.rs:194
+      const bool use = act && acc && L.y != p;
+      if (use) {
+        const double inv = rsqrt(d2 + eps2);
+        const double w = A64.w * (inv * inv * inv);
+        ax = fma(rx, w, ax);
+        ay = fma(ry, w, ay);
+        az = fma(rz, w, az);
       }
-      if (leaf) {
-        // Bucket leaf opened: exact pairs with its bodies.
-        if (__any_sync(0xffffffffu, open)) {
-          for (int q = lk.y; q < lk.z; ++q) {
-            const bool use = open && q != p;
-            if (kF32) {
-              const float4 h = body_hi[q], l = body_lo[q];
-              if (use) pair32(h, l);
-            } else {
-              const double4 b = body64[q];
-              if (use) pair64(b);
+      ninter += use;
+    }
+    const bool open = act && !acc;
+    int nxt = L.x;
+    if (__any_sync(0xffffffffu, open)) {
+      if (L.w & kWLeaf) {
+        // Bucket leaf opened: exact pairs with its bodies (skipping self).
+        const int q1 = L.z + (L.w >> 8);
+        for (int q = L.z; q < q1; ++q) {
+          const bool use = open && q != p;
+          if (kF32) {
+            const float4 h = body_hi[q], l = body_lo[q];
+            const float rx = (h.x - thx) + (l.x - tlx);
+            const float ry = (h.y - thy) + (l.y - tly);
+            const float rz = (h.z - thz) + (l.z - tlz);
+            const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2f))));
+            const float w = use ? h.w * (inv * inv * inv) : 0.f;
+            px = fmaf(rx, w, px);
+            py = fmaf(ry, w, py);
+            pz = fmaf(rz, w, pz);
+          } else {
+            const double4 b = body64[q];
+            if (use) {
+              const double rx = b.x - tx, ry = b.y - ty, rz = b.z - tz;
+              const double inv = rsqrt(fma(rx, rx, fma(ry, ry, fma(rz, rz, eps2))));
+              const double w = b.w * (inv * inv * inv);
+              ax = fma(rx, w, ax);
+              ay = fma(ry, w, ay);
+              az = fma(rz, w, az);
             }
-            ninter += use;
           }
+          ninter += use;
         }
-        node = lk.x;
       } else {
         if (open) open_to = d + 1;
-        node = __any_sync(0xffffffffu, open) ? node + 1 : lk.x;
+        nxt = nd + 1;
       }
     }
-    if (kF32 && ((++iter & 15u) == 0u)) flush();
+    return max(nxt, nd + 1);
+  };
+
+  // Sixteen visits per flush of the f32 partial sums into the compensated
+  // accumulator.
+  while (node < nnodes) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      if (node >= nnodes) break;
+      node = visit(node);
+    }
+    if (kF32) flush();
   }
   warp_count(ninter, counter);
   if (!valid) return;
@@ -326,13 +324,13 @@ int bh_walk(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force,
     PHYS_LAUNCH(c, walk_exact_kernel, grid, kWalkBlock, 0, n, t.nnodes, t.link, t.rec64, t.body64,
                 t.perm, t.hdr, p->G, eps2, (int)want_force, ox, oy, oz, c->d_counter, c->d_status);
   } else if (p->precision == PHYS_F64) {
-    PHYS_LAUNCH(c, walk_kernel<false>, grid, kWalkBlock, 0, n, t.nnodes, t.link, t.rec64, t.rec_hi,
-                t.rec_lo, t.body64, t.body_hi, t.body_lo, t.perm, t.hdr, p->G, eps2,
-                (int)want_force, p->leaf_cap, ox, oy, oz, c->d_counter, c->d_status);
+    PHYS_LAUNCH(c, walk_kernel<false>, grid, kWalkBlock, 0, (int)n, (int)t.nnodes, t.w32, t.w64,
+                t.body64, t.body_hi, t.body_lo, t.perm, t.hdr, p->G, eps2, (int)want_force, ox, oy,
+                oz, c->d_counter, c->d_status);
   } else {
-    PHYS_LAUNCH(c, walk_kernel<true>, grid, kWalkBlock, 0, n, t.nnodes, t.link, t.rec64, t.rec_hi,
-                t.rec_lo, t.body64, t.body_hi, t.body_lo, t.perm, t.hdr, p->G, eps2,
-                (int)want_force, p->leaf_cap, ox, oy, oz, c->d_counter, c->d_status);
+    PHYS_LAUNCH(c, walk_kernel<true>, grid, kWalkBlock, 0, (int)n, (int)t.nnodes, t.w32, t.w64,
+                t.body64, t.body_hi, t.body_lo, t.perm, t.hdr, p->G, eps2, (int)want_force, ox, oy,
+                oz, c->d_counter, c->d_status);
   }
   PHYS_CUDA(c, cudaEventRecord(c->ev[7], c->stream));
   return PHYS_OK;

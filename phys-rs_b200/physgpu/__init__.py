@@ -37,7 +37,7 @@ EXPORTED = [
     "phys_state_set_accel", "phys_state_download", "phys_state_size", "phys_component_write",
     "phys_component_read", "phys_gravity_forces", "phys_gravity_accel", "phys_verlet_steps",
     "phys_vv_position_step", "phys_vv_velocity_step", "phys_verlet_steps_async",
-    "phys_diagnostics", "phys_bh_export", "phys_probe_peaks",
+    "phys_diagnostics", "phys_bh_export", "phys_probe_peaks", "phys_direct_accel_targets",
 ]
 
 
@@ -109,6 +109,7 @@ def load_library(path=None):
         "phys_bh_export": ([_VP, P, i64, _I64, _I32, _I64, _D, _D, _I64, _I64, _U64, _U64, _I64,
                             _D], ctypes.c_int),
         "phys_probe_peaks": ([_VP, _D, _D], ctypes.c_int),
+        "phys_direct_accel_targets": ([_VP, P, i64, _I64, _D, _D, _D], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -245,6 +246,15 @@ class Context:
         self._check(self.lib.phys_gravity_accel(self.h, ctypes.byref(params),
                                                 *[_p(a) for a in A]), "phys_gravity_accel")
         return np.stack(A, axis=1) if download else None
+
+    def direct_accel_targets(self, params, targets):
+        """f64 direct-sum accelerations for the given targets (all sources)."""
+        t = np.ascontiguousarray(targets, dtype=np.int64)
+        out = [np.empty(t.shape[0]) for _ in range(3)]
+        self._check(self.lib.phys_direct_accel_targets(self.h, ctypes.byref(params), t.shape[0],
+                                                       _p(t, _I64), *[_p(a) for a in out]),
+                    "phys_direct_accel_targets")
+        return np.stack(out, axis=1)
 
     def verlet_steps(self, params, dt, nsteps):
         self._check(self.lib.phys_verlet_steps(self.h, ctypes.byref(params), float(dt),

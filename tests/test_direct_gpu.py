@@ -152,3 +152,17 @@ def test_bad_arguments(ctx):
         with pytest.raises(physgpu.PhysError) as ei:
             ctx.gravity_forces(bad)
         assert ei.value.status == physgpu.ERR_ARG
+
+
+def test_direct_targets_subset(ctx):
+    """Direct sum for a list of targets (the f64 reference for BH runs)."""
+    pos, _, m = ics.plummer(5000, seed=21)
+    ctx.upload(pos, None, m)
+    t = np.random.default_rng(0).choice(5000, 300, replace=False)
+    ref = oracle.accel(oracle.direct_forces(pos, m, 1.0, 0.01), m)[t]
+    a = ctx.direct_accel_targets(make_params(1.0, 0.01, precision=F64_EXACT), t)
+    assert np.array_equal(a, ref)
+    a64 = ctx.direct_accel_targets(make_params(1.0, 0.01, precision=F64), t)
+    assert rel_err(a64, ref).max() < 1e-12
+    with pytest.raises(physgpu.PhysError):
+        ctx.direct_accel_targets(make_params(1.0, 0.01, precision=F64), np.array([0, 5000]))
