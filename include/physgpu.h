@@ -169,6 +169,30 @@ int phys_vv_velocity_step(phys_ctx* ctx, double dt);
  * context's stream (host sync only for the BH node count). */
 int phys_verlet_steps_async(phys_ctx* ctx, const phys_params* p, double dt, int64_t nsteps);
 
+/* ---- batched ensemble of independent small systems ------------------- */
+/* Thousands of independent systems (1..64 bodies each) in CSR layout:
+ * system s owns bodies [offsets[s], offsets[s+1]), offsets[0] == 0.  Each
+ * system evolves under the reference's direct-sum Velocity-Verlet tick
+ * (gravity.rs:53-69, integrators.rs:63-118) with no coupling between
+ * systems.  Loading invalidates the cached accelerations. */
+int phys_ensemble_load(phys_ctx* ctx, int64_t nsys, const int64_t* offsets, const double* x,
+                       const double* y, const double* z, const double* vx, const double* vy,
+                       const double* vz, const double* m);
+/* nsteps ticks of every system in persistent kernels (one launch per
+ * `chunk` steps, 0 = all steps in one launch), the launches captured in a
+ * CUDA graph.  group = lanes per system (8, 16, 32) or 0 for the autotuned
+ * value (autotuning on first use).  p->precision: F64_EXACT or F32C; method
+ * and theta are ignored. */
+int phys_ensemble_run(phys_ctx* ctx, const phys_params* p, double dt, int64_t nsteps,
+                      int32_t group, int64_t chunk);
+int phys_ensemble_download(phys_ctx* ctx, double* x, double* y, double* z, double* vx,
+                           double* vy, double* vz, double* ax, double* ay, double* az);
+/* Times probe_steps steps for group sizes 8, 16, 32 from the current state
+ * (restored afterwards), keeps the fastest for later runs; ms3 (optional)
+ * receives the three timings. */
+int phys_ensemble_autotune(phys_ctx* ctx, const phys_params* p, double dt, int64_t probe_steps,
+                           int32_t* best_group, double* ms3);
+
 /* ---- diagnostics (src/physics/energy.rs:21-56, integrators.rs:123-129) -- */
 /* out[0] = kinetic energy sum 1/2 m v^2, out[1] = unsoftened potential energy
  * -sum_{i<j} G m_i m_j / r (r^2 == 0 pairs skipped), out[2..4] = total linear
@@ -192,8 +216,10 @@ int phys_bh_export(phys_ctx* ctx, const phys_params* p, int64_t cap, int64_t* nn
                    uint64_t* keys_lo, int64_t* perm, double* root4);
 
 /* ---- measured pipe peaks (roofline denominators) ----------------------- */
-/* Times FFMA / DFMA loops on every SM; returns TFLOP/s counting an FMA as 2. */
-int phys_probe_peaks(phys_ctx* ctx, double* fp32_tflops, double* fp64_tflops);
+/* Times FFMA, packed FFMA2 (f32x2) and DFMA loops on every SM; returns
+ * TFLOP/s counting an FMA as 2 flops (FFMA2 as 4). */
+int phys_probe_peaks(phys_ctx* ctx, double* fp32_tflops, double* fp32x2_tflops,
+                     double* fp64_tflops);
 
 #ifdef __cplusplus
 }

@@ -40,6 +40,18 @@ struct __align__(16) Rec32 {
   float4 b;  // x_lo, y_lo, z_lo, ropen2 = s_d^2 / theta^2 (-1: one-body leaf, always taken)
   int4 l;
 };
+// Paired F32C record for the two-targets-per-lane walk: every value stored
+// twice so packed f32x2 instructions take it straight from the load.
+struct __align__(16) Rec32x2 {
+  float4 q0;  // x_hi, x_hi, y_hi, y_hi
+  float4 q1;  // z_hi, z_hi, mass, mass
+  float4 q2;  // x_lo, x_lo, y_lo, y_lo
+  float4 q3;  // z_lo, z_lo, ropen2, ropen2
+  int4 l;
+};
+struct __align__(16) Body32x2 {
+  float4 q0, q1, q2, q3;  // same layout, ropen2 slot unused
+};
 struct __align__(16) Rec64 {
   double4 a;  // x, y, z, mass
   int4 l;
@@ -52,6 +64,8 @@ struct BhTree {
   const int4* link = nullptr;
   const double4* rec64 = nullptr;     // exact walk: record per node (with `link`)
   const Rec32* w32 = nullptr;         // F32C walk records
+  const Rec32x2* w32x2 = nullptr;     // F32C paired walk records
+  const Body32x2* body2 = nullptr;    // sorted bodies, paired layout
   const Rec64* w64 = nullptr;         // F64 walk records
   const double4* mc = nullptr;
   const uint32_t* perm = nullptr;     // sorted position -> caller index

@@ -61,6 +61,11 @@ struct phys_ctx {
   phys_params accel_params{};
   bool last_eval_bh = false;   // the interaction count lives in d_counter
 
+  // ---- batched ensemble (independent small systems) ----
+  int64_t ens_nsys = 0, ens_nbody = 0;
+  bool ens_accel_valid = false;
+  int ens_group = 0;           // autotuned group size (0: not tuned)
+
   // ---- small device scalars ----
   int32_t* d_status = nullptr;               // kStat* bits
   unsigned long long* d_counter = nullptr;   // interaction counter
@@ -86,6 +91,13 @@ int fail(phys_ctx* c, int code, const char* fmt, ...);
 int cuda_fail(phys_ctx* c, cudaError_t e, const char* what);
 // Ensure workspace slot `slot` holds at least `bytes`; returns device pointer.
 void* ws_get(phys_ctx* c, int slot, size_t bytes, int* status);
+// Typed form: *out = workspace slot with room for `count` T; returns a status.
+template <class T>
+int ws_alloc(phys_ctx* c, int slot, int64_t count, T** out) {
+  int st = 0;
+  *out = static_cast<T*>(ws_get(c, slot, sizeof(T) * (size_t)(count > 0 ? count : 1), &st));
+  return st;
+}
 int ensure_pinned(phys_ctx* c, size_t bytes);
 int check_launch(phys_ctx* c, const char* what);
 int read_status(phys_ctx* c, int32_t* out);
@@ -126,9 +138,19 @@ int verlet_kick_drift(phys_ctx* c, double dt);
 int flatten_sectors(phys_ctx* c, const int64_t* dsx, const int64_t* dsy, const int64_t* dsz,
                     const double* dlx, const double* dly, const double* dlz, double sector_size,
                     int bh_quirk);
+// ensemble.cu
+int ensemble_load(phys_ctx* c, int64_t nsys, const int64_t* off, const double* x, const double* y,
+                  const double* z, const double* vx, const double* vy, const double* vz,
+                  const double* m);
+int ensemble_run(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, int G,
+                 int64_t chunk);
+int ensemble_download(phys_ctx* c, double* x, double* y, double* z, double* vx, double* vy,
+                      double* vz, double* ax, double* ay, double* az);
+int ensemble_autotune(phys_ctx* c, const phys_params* p, double dt, int64_t probe_steps,
+                      int32_t* best, double* ms3);
 // diag.cu
 int diagnostics(phys_ctx* c, double G, double* out5);
-int probe_peaks(phys_ctx* c, double* fp32, double* fp64);
+int probe_peaks(phys_ctx* c, double* fp32, double* fp32x2, double* fp64);
 }  // namespace phys
 
 #define PHYS_LAUNCH(c, kernel, grid, block, smem, ...)                     \

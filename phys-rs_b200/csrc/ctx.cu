@@ -437,7 +437,7 @@ int phys_component_write(phys_ctx* c, int32_t comp, const double* a, const doubl
                          const double* d) {
   if (!c) return PHYS_ERR_ARG;
   if (c->n == 0) return fail(c, PHYS_ERR_STATE, "no body state uploaded");
-  double *da, *db, *dd;
+  double *da = nullptr, *db = nullptr, *dd = nullptr;
   PHYS_TRY(comp_ptrs(c, comp, &da, &db, &dd));
   if (!a || (db && (!b || !d))) return fail(c, PHYS_ERR_ARG, "component arrays are required");
   PHYS_TRY(h2d(c, da, a, c->n));
@@ -456,7 +456,7 @@ int phys_component_write(phys_ctx* c, int32_t comp, const double* a, const doubl
 
 int phys_component_read(phys_ctx* c, int32_t comp, double* a, double* b, double* d) {
   if (!c) return PHYS_ERR_ARG;
-  double *da, *db, *dd;
+  double *da = nullptr, *db = nullptr, *dd = nullptr;
   PHYS_TRY(comp_ptrs(c, comp, &da, &db, &dd));
   if (c->n == 0) return PHYS_OK;
   PHYS_TRY(d2h(c, a, da, c->n));
@@ -590,9 +590,55 @@ int phys_bh_export(phys_ctx* c, const phys_params* p, int64_t cap, int64_t* nnod
   return finish_status(c);
 }
 
-int phys_probe_peaks(phys_ctx* c, double* fp32, double* fp64) {
-  if (!c || !fp32 || !fp64) return PHYS_ERR_ARG;
-  return probe_peaks(c, fp32, fp64);
+int phys_ensemble_load(phys_ctx* c, int64_t nsys, const int64_t* off, const double* x,
+                       const double* y, const double* z, const double* vx, const double* vy,
+                       const double* vz, const double* m) {
+  if (!c) return PHYS_ERR_ARG;
+  if (nsys <= 0 || !off || !x || !y || !z || !m)
+    return fail(c, PHYS_ERR_ARG, "nsys > 0, offsets, positions and masses are required");
+  PHYS_CUDA(c, cudaSetDevice(c->device));
+  return ensemble_load(c, nsys, off, x, y, z, vx, vy, vz, m);
+}
+
+int phys_ensemble_run(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, int32_t group,
+                      int64_t chunk) {
+  if (!c || !p) return PHYS_ERR_ARG;
+  if (p->precision != PHYS_F64_EXACT && p->precision != PHYS_F32C)
+    return fail(c, PHYS_ERR_ARG, "ensemble precision must be F64_EXACT or F32C");
+  if (nsteps < 0 || chunk < 0) return fail(c, PHYS_ERR_ARG, "nsteps and chunk must be >= 0");
+  PHYS_TRY(reset_status(c));
+  if (group == 0) {
+    if (c->ens_group == 0) PHYS_TRY(ensemble_autotune(c, p, dt, 8, nullptr, nullptr));
+    group = c->ens_group;
+  }
+  PHYS_TRY(ensemble_run(c, p, dt, nsteps, group, chunk));
+  c->tm.walk_ms = ev_ms(c->ev[6], c->ev[7]);
+  c->last_eval_bh = false;
+  int32_t sw = 0;
+  PHYS_TRY(read_status(c, &sw));
+  if (sw & kStatOverflow) return fail(c, PHYS_ERR_ARG, "system larger than 64 bodies");
+  if (sw & kStatNonfinite) return fail(c, PHYS_ERR_NONFINITE, "non-finite ensemble state");
+  return PHYS_OK;
+}
+
+int phys_ensemble_download(phys_ctx* c, double* x, double* y, double* z, double* vx, double* vy,
+                           double* vz, double* ax, double* ay, double* az) {
+  if (!c) return PHYS_ERR_ARG;
+  if (c->ens_nsys <= 0) return fail(c, PHYS_ERR_STATE, "no ensemble loaded");
+  return ensemble_download(c, x, y, z, vx, vy, vz, ax, ay, az);
+}
+
+int phys_ensemble_autotune(phys_ctx* c, const phys_params* p, double dt, int64_t probe_steps,
+                           int32_t* best, double* ms3) {
+  if (!c || !p) return PHYS_ERR_ARG;
+  if (probe_steps <= 0) return fail(c, PHYS_ERR_ARG, "probe_steps must be > 0");
+  PHYS_TRY(reset_status(c));
+  return ensemble_autotune(c, p, dt, probe_steps, best, ms3);
+}
+
+int phys_probe_peaks(phys_ctx* c, double* fp32, double* fp32x2, double* fp64) {
+  if (!c || !fp32 || !fp32x2 || !fp64) return PHYS_ERR_ARG;
+  return probe_peaks(c, fp32, fp32x2, fp64);
 }
 
 }  // extern "C"

@@ -123,6 +123,21 @@ __global__ void ffma_probe(int iters, float seed, float* out) {
   if (s == 12345.678f) out[0] = s;  // keeps the chains live
 }
 
+__global__ void ffma2_probe(int iters, float seed, float* out) {
+  float2 a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = make_float2(seed + k * 1e-3f, seed - k * 1e-3f + threadIdx.x * 1e-7f);
+  const float2 b = make_float2(0.999999f, 0.999998f), c = make_float2(1e-7f, 2e-7f);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = __ffma2_rn(a[k], b, c);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += a[k].x + a[k].y;
+  if (s == 12345.678f) out[0] = s;
+}
+
 __global__ void dfma_probe(int iters, double seed, double* out) {
   double a[8];
 #pragma unroll
@@ -158,7 +173,7 @@ int diagnostics(phys_ctx* c, double G, double* out5) {
   return PHYS_OK;
 }
 
-int probe_peaks(phys_ctx* c, double* fp32, double* fp64) {
+int probe_peaks(phys_ctx* c, double* fp32, double* fp32x2, double* fp64) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
   const int blocks = sms * 8, threads = 256;
@@ -176,6 +191,13 @@ int probe_peaks(phys_ctx* c, double* fp32, double* fp64) {
   PHYS_CUDA(c, cudaEventSynchronize(e1));
   PHYS_CUDA(c, cudaEventElapsedTime(&ms, e0, e1));
   *fp32 = 2.0 * 8.0 * it32 * (double)blocks * threads / (ms * 1e-3) / 1e12;
+  PHYS_LAUNCH(c, ffma2_probe, blocks, threads, 0, 256, 1.0f, (float*)scratch);
+  PHYS_CUDA(c, cudaEventRecord(e0, c->stream));
+  PHYS_LAUNCH(c, ffma2_probe, blocks, threads, 0, it32, 1.0f, (float*)scratch);
+  PHYS_CUDA(c, cudaEventRecord(e1, c->stream));
+  PHYS_CUDA(c, cudaEventSynchronize(e1));
+  PHYS_CUDA(c, cudaEventElapsedTime(&ms, e0, e1));
+  *fp32x2 = 4.0 * 8.0 * it32 * (double)blocks * threads / (ms * 1e-3) / 1e12;
   PHYS_LAUNCH(c, dfma_probe, blocks, threads, 0, 64, 1.0, (double*)scratch);
   PHYS_CUDA(c, cudaEventRecord(e0, c->stream));
   PHYS_LAUNCH(c, dfma_probe, blocks, threads, 0, it64, 1.0, (double*)scratch);

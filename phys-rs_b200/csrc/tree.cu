@@ -205,7 +205,8 @@ gather_sorted_kernel(int64_t n, const uint32_t* __restrict__ perm, const uint64_
                      const double* __restrict__ x, const double* __restrict__ y,
                      const double* __restrict__ z, const double* __restrict__ m,
                      uint64_t* __restrict__ lo_s, double4* __restrict__ body64,
-                     float4* __restrict__ body_hi, float4* __restrict__ body_lo) {
+                     float4* __restrict__ body_hi, float4* __restrict__ body_lo,
+                     Body32x2* __restrict__ body2) {
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
        p += (int64_t)gridDim.x * blockDim.x) {
     const uint32_t i = perm[p];
@@ -221,6 +222,14 @@ gather_sorted_kernel(int64_t n, const uint32_t* __restrict__ perm, const uint64_
       l.w = 0.f;
       body_hi[p] = h;
       body_lo[p] = l;
+      if (body2) {
+        Body32x2 q;
+        q.q0 = make_float4(h.x, h.x, h.y, h.y);
+        q.q1 = make_float4(h.z, h.z, h.w, h.w);
+        q.q2 = make_float4(l.x, l.x, l.y, l.y);
+        q.q3 = make_float4(l.z, l.z, 0.f, 0.f);
+        body2[p] = q;
+      }
     }
   }
 }
@@ -519,7 +528,8 @@ com_recurrence_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
 __global__ void __launch_bounds__(kBlock)
 finalize_kernel(int64_t nnodes, int4* __restrict__ link, double4* __restrict__ mc, int sums,
                 int leaf_cap, const double4* __restrict__ body64, const TreeHeader* __restrict__ hdr,
-                double4* __restrict__ rec64, Rec32* __restrict__ w32, Rec64* __restrict__ w64) {
+                double4* __restrict__ rec64, Rec32* __restrict__ w32, Rec64* __restrict__ w64,
+                Rec32x2* __restrict__ w32x2) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnodes;
        k += (int64_t)gridDim.x * blockDim.x) {
     int4 lk = link[k];
@@ -556,7 +566,7 @@ finalize_kernel(int64_t nnodes, int4* __restrict__ link, double4* __restrict__ m
       o.l = wl;
       w64[k] = o;
     }
-    if (w32) {
+    if (w32 || w32x2) {
       Rec32 o;
       split_df(r.x, o.a.x, o.b.x);
       split_df(r.y, o.a.y, o.b.y);
@@ -565,7 +575,16 @@ finalize_kernel(int64_t nnodes, int4* __restrict__ link, double4* __restrict__ m
       // accept iff s^2 < theta^2 d^2  <=>  d^2 > s^2 / theta^2 (inf for theta = 0)
       o.b.w = self >= 0 ? -1.0f : (float)(hdr->s2[d] / hdr->theta2);
       o.l = wl;
-      w32[k] = o;
+      if (w32) w32[k] = o;
+      if (w32x2) {
+        Rec32x2 q;
+        q.q0 = make_float4(o.a.x, o.a.x, o.a.y, o.a.y);
+        q.q1 = make_float4(o.a.z, o.a.z, o.a.w, o.a.w);
+        q.q2 = make_float4(o.b.x, o.b.x, o.b.y, o.b.y);
+        q.q3 = make_float4(o.b.z, o.b.z, o.b.w, o.b.w);
+        q.l = wl;
+        w32x2[k] = q;
+      }
     }
   }
 }
@@ -577,24 +596,34 @@ finalize_kernel(int64_t nnodes, int4* __restrict__ link, double4* __restrict__ m
 int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t) {
   const int64_t n = c->n;
   const bool exact = p->precision == PHYS_F64_EXACT;
-  int st = PHYS_OK;
-#define WS(T, slot, count) (T*)ws_get(c, slot, sizeof(T) * (size_t)(count), &st); if (st) return st
-  uint64_t* khi = WS(uint64_t, WS_KEYS_HI, n);
-  uint64_t* klo = WS(uint64_t, WS_KEYS_LO, n);
-  uint32_t* idx = WS(uint32_t, WS_IDX, n);
-  uint64_t* khi_alt = WS(uint64_t, WS_KEYS_HI_ALT, n);
-  uint32_t* idx_alt = WS(uint32_t, WS_IDX_ALT, n);
-  uint64_t* lo_s = WS(uint64_t, WS_ENS7, n);
-  double4* body64 = WS(double4, WS_BODY_PM, n);
+  uint64_t* khi = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_KEYS_HI, n, &khi));
+  uint64_t* klo = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_KEYS_LO, n, &klo));
+  uint32_t* idx = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_IDX, n, &idx));
+  uint64_t* khi_alt = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_KEYS_HI_ALT, n, &khi_alt));
+  uint32_t* idx_alt = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_IDX_ALT, n, &idx_alt));
+  uint64_t* lo_s = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_ENS7, n, &lo_s));
+  double4* body64 = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_BODY_PM, n, &body64));
   float4* body_hi = nullptr;
   float4* body_lo = nullptr;
+  Body32x2* body2 = nullptr;
   if (need_f32) {
-    body_hi = WS(float4, WS_BODY_HI, n);
-    body_lo = WS(float4, WS_BODY_LO, n);
+    PHYS_TRY(ws_alloc(c, WS_BODY_HI, n, &body_hi));
+    PHYS_TRY(ws_alloc(c, WS_BODY_LO, n, &body_lo));
+    PHYS_TRY(ws_alloc(c, WS_ENS6, n, &body2));
   }
-  int32_t* L = WS(int32_t, WS_LCP, n + 1);
-  int32_t* cnt = WS(int32_t, WS_NCOUNT, n + 1);
-  int32_t* first = WS(int32_t, WS_NFIRST, n + 1);
+  int32_t* L = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_LCP, n + 1, &L));
+  int32_t* cnt = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_NCOUNT, n + 1, &cnt));
+  int32_t* first = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_NFIRST, n + 1, &first));
   if (!c->d_partials || c->partials_cap < 6 * kBboxGrid) {
     if (c->d_partials) cudaFree(c->d_partials);
     c->d_partials = nullptr;
@@ -617,7 +646,7 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t) {
   uint32_t* spare = in_alt ? idx : idx_alt;
   PHYS_LAUNCH(c, run_fixup_kernel, grid_for(n), kBlock, 0, n, hs, perm, klo, spare);
   PHYS_LAUNCH(c, gather_sorted_kernel, grid_for(n), kBlock, 0, n, perm, klo, c->x, c->y, c->z,
-              c->m, lo_s, body64, body_hi, body_lo);
+              c->m, lo_s, body64, body_hi, body_lo, body2);
   PHYS_CUDA(c, cudaEventRecord(c->ev[5], c->stream));
   PHYS_LAUNCH(c, lcp_count_kernel, grid_for(n + 1), kBlock, 0, n, hs, lo_s, c->d_hdr, L, cnt);
   PHYS_TRY(scan_exclusive_i32(c, cnt, first, n + 1));
@@ -632,9 +661,12 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t) {
   if (nfull < 1 || nfull > (int64_t)n * (kMaxLevels + 1))
     return fail(c, PHYS_ERR_CUDA, "tree build produced %lld nodes for %lld bodies",
                 (long long)nfull, (long long)n);
-  int4* link_full = WS(int4, WS_LINK2, nfull);
-  int32_t* parent = WS(int32_t, WS_PARENT, nfull + 1);
-  int32_t* nchild = WS(int32_t, WS_ARRIVE, 2 * (nfull + 1));
+  int4* link_full = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_LINK2, nfull, &link_full));
+  int32_t* parent = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_PARENT, nfull + 1, &parent));
+  int32_t* nchild = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_ARRIVE, 2 * (nfull + 1), &nchild));
   int32_t* arrive = nchild + (nfull + 1);
   PHYS_LAUNCH(c, emit_nodes_kernel, grid_for(n), kBlock, 0, n, hs, lo_s, L, cnt, first, c->d_hdr,
               link_full);
@@ -643,8 +675,10 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t) {
   if (p->leaf_cap > 1) {
     PHYS_LAUNCH(c, children_kernel, grid_for(nfull), kBlock, 0, nfull, link_full, parent, nchild,
                 c->d_status);
-    int32_t* keep = WS(int32_t, WS_KEEP, nfull + 1);
-    int32_t* newid = WS(int32_t, WS_NEWID, nfull + 1);
+    int32_t* keep = nullptr;
+    PHYS_TRY(ws_alloc(c, WS_KEEP, nfull + 1, &keep));
+    int32_t* newid = nullptr;
+    PHYS_TRY(ws_alloc(c, WS_NEWID, nfull + 1, &newid));
     PHYS_LAUNCH(c, keep_kernel, grid_for(nfull + 1), kBlock, 0, nfull, link_full, parent,
                 p->leaf_cap, keep);
     PHYS_TRY(scan_exclusive_i32(c, keep, newid, nfull + 1));
@@ -652,16 +686,19 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t) {
                                  c->stream));
     PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
     nnodes = hsm[0];
-    link = WS(int4, WS_LINK, nnodes);
+    PHYS_TRY(ws_alloc(c, WS_LINK, nnodes, &link));
     PHYS_LAUNCH(c, compact_kernel, grid_for(nfull), kBlock, 0, nfull, link_full, keep, newid,
                 p->leaf_cap, link);
   }
   PHYS_LAUNCH(c, children_kernel, grid_for(nnodes), kBlock, 0, nnodes, link, parent, nchild,
               c->d_status);
-  double4* mc = WS(double4, WS_NODE_S, nnodes);
+  double4* mc = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_NODE_S, nnodes, &mc));
   if (exact) {
-    int32_t* ncnt = WS(int32_t, WS_KEEP, nnodes + 1);
-    int32_t* eoff = WS(int32_t, WS_EOFF, nnodes + 1);
+    int32_t* ncnt = nullptr;
+    PHYS_TRY(ws_alloc(c, WS_KEEP, nnodes + 1, &ncnt));
+    int32_t* eoff = nullptr;
+    PHYS_TRY(ws_alloc(c, WS_EOFF, nnodes + 1, &eoff));
     PHYS_LAUNCH(c, node_count_kernel, grid_for(nnodes + 1), kBlock, 0, nnodes, link, ncnt);
     PHYS_TRY(scan_exclusive_i32(c, ncnt, eoff, nnodes + 1));
     PHYS_CUDA(c, cudaMemcpyAsync(hsm, eoff + nnodes, sizeof(int32_t), cudaMemcpyDeviceToHost,
@@ -670,8 +707,10 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t) {
     const int64_t total = (uint32_t)hsm[0];
     if (total <= 0 || total >= (int64_t(1) << 31))
       return fail(c, PHYS_ERR_ARG, "exact centre of mass needs < 2^31 (cell, body) pairs");
-    uint64_t* ent = WS(uint64_t, WS_ENTRIES, total);
-    uint64_t* ent_alt = WS(uint64_t, WS_ENTRIES_ALT, total);
+    uint64_t* ent = nullptr;
+    PHYS_TRY(ws_alloc(c, WS_ENTRIES, total, &ent));
+    uint64_t* ent_alt = nullptr;
+    PHYS_TRY(ws_alloc(c, WS_ENTRIES_ALT, total, &ent_alt));
     PHYS_LAUNCH(c, expand_kernel, grid_for(total), kBlock, 0, total, nnodes, eoff, link, perm, ent);
     int bits_b = 1, bits_n = 1;
     while ((int64_t(1) << bits_b) < n) ++bits_b;
@@ -692,14 +731,19 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t) {
   double4* rec64 = nullptr;
   Rec32* w32 = nullptr;
   Rec64* w64 = nullptr;
-  if (exact) rec64 = WS(double4, WS_NODE_PM, nnodes);
-  if (need_f32)
-    w32 = WS(Rec32, WS_NODE_HI, nnodes);
+  Rec32x2* w32x2 = nullptr;
+  if (exact) PHYS_TRY(ws_alloc(c, WS_NODE_PM, nnodes, &rec64));
+#ifndef WALK_PAIRED
+#define WALK_PAIRED 1
+#endif
+  if (need_f32 && WALK_PAIRED)
+    PHYS_TRY(ws_alloc(c, WS_NODE_HI, nnodes, &w32x2));
+  else if (need_f32)
+    PHYS_TRY(ws_alloc(c, WS_NODE_HI, nnodes, &w32));
   else if (!exact)
-    w64 = WS(Rec64, WS_NODE_LO, nnodes);
+    PHYS_TRY(ws_alloc(c, WS_NODE_LO, nnodes, &w64));
   PHYS_LAUNCH(c, finalize_kernel, grid_for(nnodes), kBlock, 0, nnodes, link, mc, exact ? 0 : 1,
-              p->leaf_cap, body64, c->d_hdr, rec64, w32, w64);
-#undef WS
+              p->leaf_cap, body64, c->d_hdr, rec64, w32, w64, w32x2);
   t->n = n;
   t->nnodes = nnodes;
   t->leaf_cap = p->leaf_cap;
@@ -707,6 +751,8 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t) {
   t->rec64 = rec64;
   t->w32 = w32;
   t->w64 = w64;
+  t->w32x2 = w32x2;
+  t->body2 = body2;
   t->mc = mc;
   t->perm = perm;
   t->body64 = body64;

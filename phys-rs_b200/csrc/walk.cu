@@ -23,6 +23,16 @@
 //              into a (hi, lo) accumulator with two-sum every 16 nodes.
 #include "bh.cuh"
 
+#ifndef WALK_BRANCHY
+#define WALK_BRANCHY 0
+#endif
+#ifndef WALK_PAIRED
+#define WALK_PAIRED 1
+#endif
+#ifndef WALK_UNROLL
+#define WALK_UNROLL 0
+#endif
+
 namespace phys {
 namespace {
 
@@ -118,11 +128,21 @@ walk_kernel(int n, int nnodes, const Rec32* __restrict__ w32, const Rec64* __res
       const float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
       acc = d2 > B.w;  // one-body leaves carry -1: always an exact pair
       const bool use = act && acc && L.y != p;
+#if WALK_BRANCHY
+      if (use) {
+        const float inv = rsqrtf(d2 + eps2f);
+        const float w = A.w * (inv * inv * inv);
+        px = fmaf(rx, w, px);
+        py = fmaf(ry, w, py);
+        pz = fmaf(rz, w, pz);
+      }
+#else
       const float inv = rsqrtf(d2 + eps2f);
       const float w = use ? A.w * (inv * inv * inv) : 0.f;
       px = fmaf(rx, w, px);
       py = fmaf(ry, w, py);
       pz = fmaf(rz, w, pz);
+#endif
       ninter += use;
     } else {
       const double rx = A64.x - tx, ry = A64.y - ty, rz = A64.z - tz;
@@ -179,14 +199,22 @@ walk_kernel(int n, int nnodes, const Rec32* __restrict__ w32, const Rec64* __res
 
   // Sixteen visits per flush of the f32 partial sums into the compensated
   // accumulator.
+#if WALK_UNROLL
   while (node < nnodes) {
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
+    for (int k = 0; k < WALK_UNROLL; ++k) {
       if (node >= nnodes) break;
       node = visit(node);
     }
     if (kF32) flush();
   }
+#else
+  unsigned iter = 0;
+  while (node < nnodes) {
+    node = visit(node);
+    if (kF32 && ((++iter & 15u) == 0u)) flush();
+  }
+#endif
   warp_count(ninter, counter);
   if (!valid) return;
   double fx, fy, fz;
@@ -209,6 +237,138 @@ walk_kernel(int n, int nnodes, const Rec32* __restrict__ w32, const Rec64* __res
   oy[i] = fy;
   oz[i] = fz;
   if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz)) atomicOr(status, kStatNonfinite);
+}
+
+// ---------------------------------------------------------------------------
+// F32C walk, two key-adjacent targets per lane (64 per warp).  The per-target
+// arithmetic runs on packed f32x2 instructions (one instruction for both
+// targets), which halves the issue slots of the floating-point work; node
+// and body records are stored pre-duplicated (x, x, y, y, ...) so the packed
+// operands come straight from the 16-byte loads.  Decisions stay per target.
+// ---------------------------------------------------------------------------
+constexpr int kWalk2Block = 128;
+
+__device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
+
+__global__ void __launch_bounds__(kWalk2Block)
+walk2_kernel(int n, int nnodes, const Rec32x2* __restrict__ w, const Body32x2* __restrict__ body2,
+             const double4* __restrict__ body64, const uint32_t* __restrict__ perm, double G,
+             double eps2, int want_force, double* __restrict__ ox, double* __restrict__ oy,
+             double* __restrict__ oz, unsigned long long* counter, int32_t* status) {
+  const int lane = threadIdx.x & 31;
+  const int base = (blockIdx.x * (kWalk2Block / 32) + (threadIdx.x >> 5)) * 64;
+  const int pa = base + 2 * lane, pb = pa + 1;
+  const bool va = pa < n, vb = pb < n;
+  float2 nhx, nhy, nhz, nlx, nly, nlz;  // negated target coordinates (a, b)
+  {
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 a0 = va ? body2[pa].q0 : z4, a1 = va ? body2[pa].q1 : z4;
+    const float4 a2 = va ? body2[pa].q2 : z4, a3 = va ? body2[pa].q3 : z4;
+    const float4 b0 = vb ? body2[pb].q0 : z4, b1 = vb ? body2[pb].q1 : z4;
+    const float4 b2 = vb ? body2[pb].q2 : z4, b3 = vb ? body2[pb].q3 : z4;
+    nhx = make_float2(-a0.x, -b0.x);
+    nhy = make_float2(-a0.z, -b0.z);
+    nhz = make_float2(-a1.x, -b1.x);
+    nlx = make_float2(-a2.x, -b2.x);
+    nly = make_float2(-a2.z, -b2.z);
+    nlz = make_float2(-a3.x, -b3.x);
+  }
+  const float eps2f = (float)eps2;
+  const float2 e2 = make_float2(eps2f, eps2f);
+  float2 px = make_float2(0.f, 0.f), py = px, pz = px;  // partial sums since last flush
+  float hxa = 0, hya = 0, hza = 0, lxa = 0, lya = 0, lza = 0;  // compensated, target a
+  float hxb = 0, hyb = 0, hzb = 0, lxb = 0, lyb = 0, lzb = 0;  // compensated, target b
+  int oa = va ? 0 : -1, ob = vb ? 0 : -1;  // opened levels on the current path
+  unsigned ninter = 0;
+
+  auto flush = [&]() {
+    float s, e;
+    two_sum(hxa, px.x, s, e); hxa = s; lxa += e;
+    two_sum(hya, py.x, s, e); hya = s; lya += e;
+    two_sum(hza, pz.x, s, e); hza = s; lza += e;
+    two_sum(hxb, px.y, s, e); hxb = s; lxb += e;
+    two_sum(hyb, py.y, s, e); hyb = s; lyb += e;
+    two_sum(hzb, pz.y, s, e); hzb = s; lzb += e;
+    px = py = pz = make_float2(0.f, 0.f);
+  };
+  // Packed separation from a paired record (q0..q3) to both targets.
+  auto sep = [&](float4 q0, float4 q1, float4 q2, float4 q3, float2& rx, float2& ry,
+                 float2& rz) {
+    rx = __fadd2_rn(__fadd2_rn(lo2(q0), nhx), __fadd2_rn(lo2(q2), nlx));
+    ry = __fadd2_rn(__fadd2_rn(hi2(q0), nhy), __fadd2_rn(hi2(q2), nly));
+    rz = __fadd2_rn(__fadd2_rn(lo2(q1), nhz), __fadd2_rn(lo2(q3), nlz));
+  };
+  auto accum = [&](float2 rx, float2 ry, float2 rz, float2 r2, float2 m2, bool ua, bool ub) {
+    const float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    float2 wg = __fmul2_rn(m2, __fmul2_rn(__fmul2_rn(inv, inv), inv));
+    wg.x = ua ? wg.x : 0.f;
+    wg.y = ub ? wg.y : 0.f;
+    px = __ffma2_rn(rx, wg, px);
+    py = __ffma2_rn(ry, wg, py);
+    pz = __ffma2_rn(rz, wg, pz);
+    ninter += (unsigned)ua + (unsigned)ub;
+  };
+
+  auto visit = [&](int nd) -> int {
+    const Rec32x2* rp = w + nd;
+    const float4 q0 = rp->q0, q1 = rp->q1, q2 = rp->q2, q3 = rp->q3;
+    const int4 L = rp->l;
+    const int d = L.w & kWDepth;
+    oa = min(oa, d);
+    ob = min(ob, d);
+    const bool acta = oa == d, actb = ob == d;
+    float2 rx, ry, rz;
+    sep(q0, q1, q2, q3, rx, ry, rz);
+    const float2 d2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __fmul2_rn(rz, rz)));
+    const bool acca = d2.x > q3.z, accb = d2.y > q3.w;  // -1 for one-body leaves
+    accum(rx, ry, rz, __fadd2_rn(d2, e2), hi2(q1), acta && acca && L.y != pa,
+          actb && accb && L.y != pb);
+    const bool opa = acta && !acca, opb = actb && !accb;
+    int nxt = L.x;
+    if (__any_sync(0xffffffffu, opa || opb)) {
+      if (L.w & kWLeaf) {
+        const int qe = L.z + (L.w >> 8);
+        for (int q = L.z; q < qe; ++q) {
+          const Body32x2* bp = body2 + q;
+          const float4 b0 = bp->q0, b1 = bp->q1, b2 = bp->q2, b3 = bp->q3;
+          float2 bx, by, bz;
+          sep(b0, b1, b2, b3, bx, by, bz);
+          const float2 r2 = __ffma2_rn(bx, bx, __ffma2_rn(by, by, __ffma2_rn(bz, bz, e2)));
+          accum(bx, by, bz, r2, hi2(b1), opa && q != pa, opb && q != pb);
+        }
+      } else {
+        if (opa) oa = d + 1;
+        if (opb) ob = d + 1;
+        nxt = nd + 1;
+      }
+    }
+    return max(nxt, nd + 1);
+  };
+
+  int node = 0;
+  unsigned iter = 0;
+  while (node < nnodes) {
+    node = visit(node);
+    if ((++iter & 15u) == 0u) flush();
+  }
+  flush();
+  warp_count(ninter, counter);
+  auto out = [&](int pp, float hx, float hy, float hz, float lx, float ly, float lz) {
+    double fx = (double)hx + (double)lx, fy = (double)hy + (double)ly,
+           fz = (double)hz + (double)lz;
+    const double sc = want_force ? G * body64[pp].w : G;
+    fx *= sc;
+    fy *= sc;
+    fz *= sc;
+    const uint32_t i = perm[pp];
+    ox[i] = fx;
+    oy[i] = fy;
+    oz[i] = fz;
+    if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz)) atomicOr(status, kStatNonfinite);
+  };
+  if (va) out(pa, hxa, hya, hza, lxa, lya, lza);
+  if (vb) out(pb, hxb, hyb, hzb, lxb, lyb, lzb);
 }
 
 // ---------------------------------------------------------------------------
@@ -327,6 +487,11 @@ int bh_walk(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force,
     PHYS_LAUNCH(c, walk_kernel<false>, grid, kWalkBlock, 0, (int)n, (int)t.nnodes, t.w32, t.w64,
                 t.body64, t.body_hi, t.body_lo, t.perm, t.hdr, p->G, eps2, (int)want_force, ox, oy,
                 oz, c->d_counter, c->d_status);
+  } else if (WALK_PAIRED && t.w32x2) {
+    const int grid2 = (int)ceil_div(n, 64 * (kWalk2Block / 32));
+    PHYS_LAUNCH(c, walk2_kernel, grid2, kWalk2Block, 0, (int)n, (int)t.nnodes, t.w32x2, t.body2,
+                t.body64, t.perm, p->G, eps2, (int)want_force, ox, oy, oz, c->d_counter,
+                c->d_status);
   } else {
     PHYS_LAUNCH(c, walk_kernel<true>, grid, kWalkBlock, 0, (int)n, (int)t.nnodes, t.w32, t.w64,
                 t.body64, t.body_hi, t.body_lo, t.perm, t.hdr, p->G, eps2, (int)want_force, ox, oy,

@@ -38,6 +38,7 @@ EXPORTED = [
     "phys_component_read", "phys_gravity_forces", "phys_gravity_accel", "phys_verlet_steps",
     "phys_vv_position_step", "phys_vv_velocity_step", "phys_verlet_steps_async",
     "phys_diagnostics", "phys_bh_export", "phys_probe_peaks", "phys_direct_accel_targets",
+    "phys_ensemble_load", "phys_ensemble_run", "phys_ensemble_download", "phys_ensemble_autotune",
 ]
 
 
@@ -78,7 +79,7 @@ def load_library(path=None):
     global _lib
     if _lib is not None:
         return _lib
-    path = path or LIB_PATH
+    path = path or os.environ.get("PHYSGPU_LIB") or LIB_PATH
     if not os.path.exists(path):
         raise PhysError(ERR_STATE, "libphysgpu.so not built (%s); run __graft_entry__.build()" % path)
     L = ctypes.CDLL(path)
@@ -108,8 +109,12 @@ def load_library(path=None):
         "phys_diagnostics": ([_VP, dbl, _D], ctypes.c_int),
         "phys_bh_export": ([_VP, P, i64, _I64, _I32, _I64, _D, _D, _I64, _I64, _U64, _U64, _I64,
                             _D], ctypes.c_int),
-        "phys_probe_peaks": ([_VP, _D, _D], ctypes.c_int),
+        "phys_probe_peaks": ([_VP, _D, _D, _D], ctypes.c_int),
         "phys_direct_accel_targets": ([_VP, P, i64, _I64, _D, _D, _D], ctypes.c_int),
+        "phys_ensemble_load": ([_VP, i64, _I64] + [_D] * 7, ctypes.c_int),
+        "phys_ensemble_run": ([_VP, P, dbl, i64, i32, i64], ctypes.c_int),
+        "phys_ensemble_download": ([_VP] + [_D] * 9, ctypes.c_int),
+        "phys_ensemble_autotune": ([_VP, P, dbl, i64, _I32, _D], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -256,6 +261,38 @@ class Context:
                     "phys_direct_accel_targets")
         return np.stack(out, axis=1)
 
+    # ---- batched ensemble ----
+    def ensemble_load(self, offsets, pos, vel, m):
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        pos = np.asarray(pos, np.float64)
+        m = np.ascontiguousarray(m, dtype=np.float64)
+        P = [_col(pos, k) for k in range(3)]
+        V = [None] * 3 if vel is None else [_col(np.asarray(vel, np.float64), k) for k in range(3)]
+        self._check(self.lib.phys_ensemble_load(self.h, off.shape[0] - 1, _p(off, _I64),
+                                                *[_p(a) for a in P], *[_p(a) for a in V], _p(m)),
+                    "phys_ensemble_load")
+        self.ens_n = m.shape[0]
+
+    def ensemble_run(self, params, dt, nsteps, group=0, chunk=0):
+        self._check(self.lib.phys_ensemble_run(self.h, ctypes.byref(params), float(dt),
+                                               int(nsteps), int(group), int(chunk)),
+                    "phys_ensemble_run")
+
+    def ensemble_download(self):
+        out = [np.empty(self.ens_n) for _ in range(9)]
+        self._check(self.lib.phys_ensemble_download(self.h, *[_p(a) for a in out]),
+                    "phys_ensemble_download")
+        st = lambda a, b, c: np.stack([a, b, c], axis=1)
+        return st(*out[0:3]), st(*out[3:6]), st(*out[6:9])
+
+    def ensemble_autotune(self, params, dt, probe_steps=8):
+        best = ctypes.c_int32()
+        ms = np.zeros(3)
+        self._check(self.lib.phys_ensemble_autotune(self.h, ctypes.byref(params), float(dt),
+                                                    int(probe_steps), ctypes.byref(best), _p(ms)),
+                    "phys_ensemble_autotune")
+        return best.value, dict(zip((8, 16, 32), ms.tolist()))
+
     def verlet_steps(self, params, dt, nsteps):
         self._check(self.lib.phys_verlet_steps(self.h, ctypes.byref(params), float(dt),
                                                int(nsteps)), "phys_verlet_steps")
@@ -281,10 +318,11 @@ class Context:
         return t.as_dict()
 
     def probe_peaks(self):
-        a, b = ctypes.c_double(), ctypes.c_double()
-        self._check(self.lib.phys_probe_peaks(self.h, ctypes.byref(a), ctypes.byref(b)),
-                    "phys_probe_peaks")
-        return a.value, b.value
+        """Measured (fp32 FFMA, fp32 packed FFMA2, fp64 DFMA) TFLOP/s."""
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.phys_probe_peaks(self.h, ctypes.byref(a), ctypes.byref(b),
+                                              ctypes.byref(c)), "phys_probe_peaks")
+        return a.value, b.value, c.value
 
     def bh_export(self, params):
         n = self.n
