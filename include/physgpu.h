@@ -24,6 +24,7 @@
 #ifndef PHYSGPU_H
 #define PHYSGPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -214,6 +215,27 @@ int phys_bh_export(phys_ctx* ctx, const phys_params* p, int64_t cap, int64_t* nn
                    int32_t* depth, int64_t* count, double* mass, double* com,
                    int64_t* leaf_body, int64_t* body_leaf, uint64_t* keys_hi,
                    uint64_t* keys_lo, int64_t* perm, double* root4);
+
+/* ---- direct sum without allocation --------------------------------------- */
+/* No counterpart in the reference.  For callers that must not allocate
+ * device memory once running: an engine tick that fixed all its buffers at
+ * start-up (cudaMalloc / cudaFree can synchronise the whole device and stall
+ * the tick), or a host application that lends this library only memory from
+ * its own pool.  Computes direct-sum accelerations
+ *   a_i = G sum_{j != i} m_j r_ij / (|r_ij|^2 + eps^2)^{3/2}
+ * for n <= 32768 bodies whose positions, masses and outputs are in the
+ * caller's DEVICE memory, on the caller's stream (NULL: default stream),
+ * precision PHYS_F64 or PHYS_F32C.  It allocates nothing: its scratch is one
+ * fixed device array of about 7.3 MiB that every GPU loading the library
+ * keeps until the process exits.  The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  All calls share the array, so calls that overlap on the
+ * GPU race: order them.  n outside 0..32768 returns PHYS_ERR_ARG with a
+ * message in errbuf (optional, errlen bytes).  Synchronous at return. */
+int phys_direct_accel_noalloc(int64_t n, const double* x, const double* y, const double* z,
+                              const double* m, double G, double eps, int32_t precision,
+                              double* ax, double* ay, double* az, void* stream, char* errbuf,
+                              size_t errlen);
 
 /* ---- measured pipe peaks (roofline denominators) ----------------------- */
 /* Times FFMA, packed FFMA2 (f32x2) and DFMA loops on every SM; returns

@@ -121,6 +121,10 @@ int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, 
                 double* oz);
 int direct_targets(phys_ctx* c, const phys_params* p, int64_t nt, const int64_t* d_tidx,
                    double* ox, double* oy, double* oz);
+int direct_accel_launch_scratch(cudaStream_t s, int64_t n, const double* x, const double* y,
+                                const double* z, const double* m, double G, double eps,
+                                int precision, int64_t nslices, double* part, float4* bh,
+                                float4* bl, int32_t* status, double* ox, double* oy, double* oz);
 // tree.cu
 int bh_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, double* oy,
             double* oz);

@@ -403,6 +403,33 @@ int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, 
   return PHYS_OK;
 }
 
+// Sliced F64 / F32C direct sum on caller-owned device buffers and stream,
+// with caller-provided scratch: `part` (3 * n * nslices doubles), `bh`/`bl`
+// (n float4 each, F32C only) and the status word.  Launches the same kernels
+// as direct_eval; allocates nothing.
+int direct_accel_launch_scratch(cudaStream_t s, int64_t n, const double* x, const double* y,
+                                const double* z, const double* m, double G, double eps,
+                                int precision, int64_t nslices, double* part, float4* bh,
+                                float4* bl, int32_t* status, double* ox, double* oy,
+                                double* oz) {
+  const double eps2 = eps * eps;
+  const int64_t slice_len = ceil_div(ceil_div(n, nslices), kTile) * kTile;
+  const int64_t nsl = ceil_div(n, slice_len);
+  dim3 grid((unsigned)ceil_div(n, kTile), (unsigned)nsl);
+  const int g = (int)min64(ceil_div(n, 256), 148 * 8);
+  if (precision == PHYS_F64) {
+    direct_f64_kernel<<<grid, kTile, 0, s>>>(n, slice_len, x, y, z, m, G, eps2, 0, ox, oy, oz,
+                                             part, status);
+  } else {
+    split_bodies_kernel<<<g, 256, 0, s>>>(n, x, y, z, m, bh, bl, status);
+    direct_f32c_kernel<<<grid, kTile, 0, s>>>(n, slice_len, bh, bl, m, G, (float)eps2, 0, ox, oy,
+                                              oz, part, status);
+  }
+  if (nsl > 1)
+    slice_reduce_kernel<<<g, 256, 0, s>>>(n, (int)nsl, part, m, G, 0, ox, oy, oz, status);
+  return cudaGetLastError() == cudaSuccess ? PHYS_OK : PHYS_ERR_CUDA;
+}
+
 int direct_targets(phys_ctx* c, const phys_params* p, int64_t nt, const int64_t* d_tidx,
                    double* ox, double* oy, double* oz) {
   const int64_t n = c->n;

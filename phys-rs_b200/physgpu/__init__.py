@@ -39,6 +39,7 @@ EXPORTED = [
     "phys_vv_position_step", "phys_vv_velocity_step", "phys_verlet_steps_async",
     "phys_diagnostics", "phys_bh_export", "phys_probe_peaks", "phys_direct_accel_targets",
     "phys_ensemble_load", "phys_ensemble_run", "phys_ensemble_download", "phys_ensemble_autotune",
+    "phys_direct_accel_noalloc",
 ]
 
 
@@ -115,6 +116,8 @@ def load_library(path=None):
         "phys_ensemble_run": ([_VP, P, dbl, i64, i32, i64], ctypes.c_int),
         "phys_ensemble_download": ([_VP] + [_D] * 9, ctypes.c_int),
         "phys_ensemble_autotune": ([_VP, P, dbl, i64, _I32, _D], ctypes.c_int),
+        "phys_direct_accel_noalloc": ([i64, _VP, _VP, _VP, _VP, dbl, dbl, i32, _VP, _VP, _VP, _VP,
+                                       ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
