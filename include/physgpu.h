@@ -194,6 +194,24 @@ int phys_ensemble_download(phys_ctx* ctx, double* x, double* y, double* z, doubl
 int phys_ensemble_autotune(phys_ctx* ctx, const phys_params* p, double dt, int64_t probe_steps,
                            int32_t* best_group, double* ms3);
 
+/* ---- trajectory gradients (hand-written adjoint) ------------------------ */
+/* No counterpart in the reference (it has no differentiation).  Loss
+ *   L = sum_i |x_i(T) - target_i|^2
+ * after nsteps Velocity-Verlet ticks (integrators.rs:63-104) of the direct
+ * sum (gravity.rs:53-69), p->precision must be PHYS_F64, started from the
+ * uploaded state (which is left unchanged).  phys_adjoint_direct returns L
+ * and dL/dx0, dL/dv0, dL/dm (each output may be NULL) by a reverse sweep
+ * through the acceleration's Jacobian and the Verlet step, checkpointing
+ * (x, v) every `checkpoint` steps and recomputing each segment.
+ * phys_trajectory_loss is the same forward pass only (finite differences). */
+int phys_adjoint_direct(phys_ctx* ctx, const phys_params* p, double dt, int64_t nsteps,
+                        int64_t checkpoint, const double* tx, const double* ty, const double* tz,
+                        double* loss, double* gx, double* gy, double* gz, double* gvx,
+                        double* gvy, double* gvz, double* gm);
+int phys_trajectory_loss(phys_ctx* ctx, const phys_params* p, double dt, int64_t nsteps,
+                         const double* tx, const double* ty, const double* tz, double* loss,
+                         double* xT, double* yT, double* zT);
+
 /* ---- diagnostics (src/physics/energy.rs:21-56, integrators.rs:123-129) -- */
 /* out[0] = kinetic energy sum 1/2 m v^2, out[1] = unsoftened potential energy
  * -sum_{i<j} G m_i m_j / r (r^2 == 0 pairs skipped), out[2..4] = total linear

@@ -152,6 +152,13 @@ int ensemble_download(phys_ctx* c, double* x, double* y, double* z, double* vx, 
                       double* vz, double* ax, double* ay, double* az);
 int ensemble_autotune(phys_ctx* c, const phys_params* p, double dt, int64_t probe_steps,
                       int32_t* best, double* ms3);
+// adjoint.cu
+int trajectory_loss(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps,
+                    const double* tx, const double* ty, const double* tz, double* loss,
+                    double* xT, double* yT, double* zT);
+int adjoint(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, int64_t K,
+            const double* tx, const double* ty, const double* tz, double* loss, double* gxyz[3],
+            double* gvxyz[3], double* gm);
 // diag.cu
 int diagnostics(phys_ctx* c, double G, double* out5);
 int probe_peaks(phys_ctx* c, double* fp32, double* fp32x2, double* fp64);

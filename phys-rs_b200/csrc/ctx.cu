@@ -636,6 +636,33 @@ int phys_ensemble_autotune(phys_ctx* c, const phys_params* p, double dt, int64_t
   return ensemble_autotune(c, p, dt, probe_steps, best, ms3);
 }
 
+int phys_adjoint_direct(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps,
+                        int64_t checkpoint, const double* tx, const double* ty, const double* tz,
+                        double* loss, double* gx, double* gy, double* gz, double* gvx,
+                        double* gvy, double* gvz, double* gm) {
+  if (!c || !loss) return PHYS_ERR_ARG;
+  PHYS_TRY(reset_status(c));
+  PHYS_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+  double* gxyz[3] = {gx, gy, gz};
+  double* gvxyz[3] = {gvx, gvy, gvz};
+  PHYS_TRY(adjoint(c, p, dt, nsteps, checkpoint, tx, ty, tz, loss, gxyz, gvxyz, gm));
+  PHYS_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+  c->last_eval_bh = false;
+  int st = finish_status(c);
+  c->tm.total_ms = ev_ms(c->ev[0], c->ev[1]);
+  return st;
+}
+
+int phys_trajectory_loss(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps,
+                         const double* tx, const double* ty, const double* tz, double* loss,
+                         double* xT, double* yT, double* zT) {
+  if (!c || !loss) return PHYS_ERR_ARG;
+  PHYS_TRY(reset_status(c));
+  PHYS_TRY(trajectory_loss(c, p, dt, nsteps, tx, ty, tz, loss, xT, yT, zT));
+  c->last_eval_bh = false;
+  return finish_status(c);
+}
+
 int phys_probe_peaks(phys_ctx* c, double* fp32, double* fp32x2, double* fp64) {
   if (!c || !fp32 || !fp32x2 || !fp64) return PHYS_ERR_ARG;
   return probe_peaks(c, fp32, fp32x2, fp64);

@@ -39,7 +39,7 @@ EXPORTED = [
     "phys_vv_position_step", "phys_vv_velocity_step", "phys_verlet_steps_async",
     "phys_diagnostics", "phys_bh_export", "phys_probe_peaks", "phys_direct_accel_targets",
     "phys_ensemble_load", "phys_ensemble_run", "phys_ensemble_download", "phys_ensemble_autotune",
-    "phys_direct_accel_noalloc",
+    "phys_direct_accel_noalloc", "phys_adjoint_direct", "phys_trajectory_loss",
 ]
 
 
@@ -116,6 +116,8 @@ def load_library(path=None):
         "phys_ensemble_run": ([_VP, P, dbl, i64, i32, i64], ctypes.c_int),
         "phys_ensemble_download": ([_VP] + [_D] * 9, ctypes.c_int),
         "phys_ensemble_autotune": ([_VP, P, dbl, i64, _I32, _D], ctypes.c_int),
+        "phys_adjoint_direct": ([_VP, P, dbl, i64, i64] + [_D] * 11, ctypes.c_int),
+        "phys_trajectory_loss": ([_VP, P, dbl, i64] + [_D] * 7, ctypes.c_int),
         "phys_direct_accel_noalloc": ([i64, _VP, _VP, _VP, _VP, dbl, dbl, i32, _VP, _VP, _VP, _VP,
                                        ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
     }
@@ -295,6 +297,33 @@ class Context:
                                                     int(probe_steps), ctypes.byref(best), _p(ms)),
                     "phys_ensemble_autotune")
         return best.value, dict(zip((8, 16, 32), ms.tolist()))
+
+    # ---- trajectory gradients ----
+    def adjoint(self, params, dt, nsteps, targets, checkpoint=32):
+        """(loss, dL/dx0 (n,3), dL/dv0 (n,3), dL/dm (n,)) by the hand-written adjoint."""
+        t = np.asarray(targets, np.float64)
+        T = [_col(t, k) for k in range(3)]
+        n = self.n
+        gx = [np.empty(n) for _ in range(3)]
+        gv = [np.empty(n) for _ in range(3)]
+        gm = np.empty(n)
+        loss = ctypes.c_double()
+        self._check(self.lib.phys_adjoint_direct(
+            self.h, ctypes.byref(params), float(dt), int(nsteps), int(checkpoint),
+            *[_p(a) for a in T], ctypes.byref(loss), *[_p(a) for a in gx], *[_p(a) for a in gv],
+            _p(gm)), "phys_adjoint_direct")
+        return loss.value, np.stack(gx, 1), np.stack(gv, 1), gm
+
+    def trajectory_loss(self, params, dt, nsteps, targets, final=False):
+        t = np.asarray(targets, np.float64)
+        T = [_col(t, k) for k in range(3)]
+        loss = ctypes.c_double()
+        X = [np.empty(self.n) for _ in range(3)] if final else [None] * 3
+        self._check(self.lib.phys_trajectory_loss(self.h, ctypes.byref(params), float(dt),
+                                                  int(nsteps), *[_p(a) for a in T],
+                                                  ctypes.byref(loss), *[_p(a) for a in X]),
+                    "phys_trajectory_loss")
+        return (loss.value, np.stack(X, 1)) if final else loss.value
 
     def verlet_steps(self, params, dt, nsteps):
         self._check(self.lib.phys_verlet_steps(self.h, ctypes.byref(params), float(dt),
