@@ -41,15 +41,30 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--workload", default="bh",
+                    choices=["bh", "galaxy", "ensemble", "direct", "adjoint"],
+                    help="bh: 2^20 Plummer Barnes-Hut (default); galaxy: 2^24 disk+halo BH; "
+                         "ensemble: 16384 small systems; direct: 1024-body direct sum; "
+                         "adjoint: 4096-body trajectory gradient")
+    ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--leaf-cap", type=int, default=8)
-    ap.add_argument("--theta", type=float, default=0.5)
-    ap.add_argument("--eps", type=float, default=0.01)
-    ap.add_argument("--dt", type=float, default=1e-3)
+    ap.add_argument("--theta", type=float, default=None)
+    ap.add_argument("--eps", type=float, default=None)
+    ap.add_argument("--dt", type=float, default=None)
+    ap.add_argument("--ens-steps", type=int, default=10000, help="ensemble steps per bench step")
     ap.add_argument("--no-extras", action="store_true", help="skip FP64 comparison and accuracy")
     ap.add_argument("--quick", action="store_true",
                     help="device-resident timing only (no e2e, extras, CPU baseline): profiling")
-    return ap.parse_args()
+    a = ap.parse_args()
+    defaults = {  # n, theta, eps, dt per workload shape
+        "bh": (1 << 20, 0.5, 0.01, 1e-3), "galaxy": (1 << 24, 0.6, 0.02, 5e-4),
+        "ensemble": (16384, 0.5, 1e-3, 1e-4), "direct": (1024, 0.5, 0.01, 1e-3),
+        "adjoint": (4096, 0.5, 0.01, 1e-3)}[a.workload]
+    a.n = a.n if a.n is not None else defaults[0]
+    a.theta = a.theta if a.theta is not None else defaults[1]
+    a.eps = a.eps if a.eps is not None else defaults[2]
+    a.dt = a.dt if a.dt is not None else defaults[3]
+    return a
 
 
 def dist_env():
@@ -132,7 +147,10 @@ def run_reference(args, ws, rank):
     if rank != 0:
         return 0
     import physgpu.ics as ics
-    pos, vel, m = ics.plummer(args.n, seed=0)
+    if args.workload == "galaxy":
+        pos, vel, m = ics.galaxy(args.n, seed=0)
+    else:
+        pos, vel, m = ics.plummer(args.n, seed=0)
     nthreads = oracle.ncpu()
     rng = np.random.default_rng(1)
     sample = 16384
@@ -165,16 +183,32 @@ def run_reference(args, ws, rank):
 
 
 def workload_config(args, precision, leaf_cap):
-    return {"workload": "barnes_hut_plummer_n%d" % args.n, "n": args.n, "theta": args.theta,
-            "eps": args.eps, "G": 1.0, "dt": args.dt, "leaf_cap": leaf_cap,
-            "precision": precision, "ics": "Plummer a=1, equal masses 1/N, seed=rank",
+    galaxy = args.workload == "galaxy"
+    return {"workload": ("barnes_hut_galaxy_n%d" if galaxy else "barnes_hut_plummer_n%d") % args.n,
+            "n": args.n, "theta": args.theta, "eps": args.eps, "G": 1.0, "dt": args.dt,
+            "leaf_cap": leaf_cap, "precision": precision,
+            "ics": ("30% exponential disk (R_d=1, sech^2 z0=0.1) + 70% NFW halo (r_s=3, cut 30), "
+                    "seed=rank" if galaxy else "Plummer a=1, equal masses 1/N, seed=rank"),
             "l2": "flushed between timed steps (256 MiB write)"}
+
+
+# DRAM bytes (read + write) of one walk launch for the default workload
+# (N = 2^20 Plummer, theta 0.5, leaf capacity 8, F32C), from one ncu capture
+# of this binary: dram__bytes_read.sum 131.8 MB + dram__bytes_write.sum 25.3 MB.
+WALK_TRAFFIC_BYTES = 157.05e6
+
+
+def walk_traffic(args):
+    if (args.workload, args.n, args.theta, args.leaf_cap) == ("bh", 1 << 20, 0.5, 8):
+        return WALK_TRAFFIC_BYTES
+    return None
 
 
 def run_ours(args, ws, rank, local):
     import torch
 
     import physgpu
+    import physgpu.dist as dist
     import physgpu.ics as ics
     from physgpu import BARNES_HUT, F32C, F64, make_params
 
@@ -188,7 +222,10 @@ def run_ours(args, ws, rank, local):
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
     flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
-    pos, vel, m = ics.plummer(args.n, seed=rank)
+    if args.workload == "galaxy":
+        pos, vel, m = ics.galaxy(args.n, seed=rank)
+    else:
+        pos, vel, m = ics.plummer(args.n, seed=rank)
     n = args.n
     p32 = make_params(1.0, args.eps, args.theta, BARNES_HUT, F32C, args.leaf_cap)
     p64 = make_params(1.0, args.eps, args.theta, BARNES_HUT, F64, args.leaf_cap)
@@ -230,10 +267,7 @@ def run_ours(args, ws, rank, local):
     barrier()
     clk = clocks.stop()
     launches = ctx.timings()["launches"] - launches0
-    t_all = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        torch.distributed.all_reduce(t_all, op=torch.distributed.ReduceOp.MAX)
-    t_max_ms = float(t_all.item())
+    t_max_ms = dist.max_over_ranks(tot_ms, device="cuda")
     value = ws * n * args.steps / (t_max_ms * 1e-3)
     tm = ctx.timings()
 
@@ -284,10 +318,8 @@ def run_ours(args, ws, rank, local):
         e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = ws * n * args.steps / (float(e2e_t.item()) * 1e-3)
+    e2e_ms = dist.max_over_ranks(e0.elapsed_time(e1), device="cuda")
+    e2e_value = ws * n * args.steps / (e2e_ms * 1e-3)
 
     extras = {}
     if not args.no_extras:
@@ -338,13 +370,13 @@ def run_ours(args, ws, rank, local):
                             "(FMA = 2 flops); ffma %.1f, ffma2 %.1f" % (fp32_tf, fp32x2_tf)),
             "flops_per_interaction": FLOPS_PER_INTERACTION,
             "interactions_per_launch": inter_med, "walk_ms": walk_med,
-            "traffic": None, "fp64_peak_tflops": fp64_tf,
+            "traffic": walk_traffic(args), "fp64_peak_tflops": fp64_tf,
             "phase_ms_last_step": {k: round(tm[k], 4) for k in
                                    ("bbox_ms", "keys_ms", "sort_ms", "tree_ms", "walk_ms")}}
 
     # ---- CPU baseline (rank 0, N=1): reference algorithm on a bounded sample ----
     cpu = None
-    if rank == 0 and ws == 1:
+    if rank == 0 and ws == 1 and args.workload == "bh":
         import oracle
         oracle.lib()
         nth = oracle.ncpu()
@@ -357,10 +389,13 @@ def run_ours(args, ws, rank, local):
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws,
+            "metric": METRIC if args.workload == "bh" else
+            "particle-steps/s, %d-body galaxy BH θ=%g, FP32-comp" % (n, args.theta),
+            "value": value, "unit": "particle-steps/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32c",
-            "data": "synthetic (seeded Plummer sphere; no dataset)",
+            "data": "synthetic (seeded %s; no dataset)" % (
+                "Plummer sphere" if args.workload == "bh" else "exponential disk + NFW halo"),
             "config": workload_config(args, "f32c (f32 pair terms, two-sum, f64 state)",
                                       args.leaf_cap),
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
@@ -377,12 +412,224 @@ def run_ours(args, ws, rank, local):
     return 0
 
 
+def _line(args, ws, metric, value, unit, ms, dtype, config, **kw):
+    d = {"metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps,
+         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+         "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded; no dataset)",
+         "config": config}
+    d.update(kw)
+    return d
+
+
+def run_other(args, ws, rank, local):
+    """Ensemble, direct-sum and adjoint workload shapes (one device per rank,
+    independent work per rank)."""
+    import torch
+
+    import physgpu
+    import physgpu.dist as dist
+    import physgpu.ics as ics
+    from physgpu import DIRECT, F32C, F64, F64_EXACT, make_params
+
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local))
+    ctx = physgpu.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    fp32_tf, fp32x2_tf, fp64_tf = ctx.probe_peaks()
+
+    def timed(fn, k):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(k)]
+        with torch.cuda.stream(stream):
+            for i in range(k):
+                evs[i][0].record(stream)
+                fn()
+                evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+
+    clocks = Clocks(local)
+    line = None
+    if args.workload == "ensemble":
+        off, pos, vel, m = ics.ensemble(args.n, seed=rank)
+        ns = np.diff(off)
+        pairs = int(np.sum(ns * (ns - 1)))
+        nb = int(off[-1])
+        p = make_params(1.0, args.eps, precision=F32C)
+        ctx.ensemble_load(off, pos, vel, m)
+        best, tune = ctx.ensemble_autotune(p, args.dt, 16)
+        for _ in range(args.warmup):
+            ctx.ensemble_run(p, args.dt, args.ens_steps, group=best)
+        barrier()
+        l0 = ctx.timings()["launches"]
+        clocks.start()
+        ms = timed(lambda: ctx.ensemble_run(p, args.dt, args.ens_steps, group=best), args.steps)
+        clk = clocks.stop()
+        t = dist.max_over_ranks(sum(ms), device="cuda")
+        value = ws * nb * args.ens_steps * args.steps / (t * 1e-3)
+        ach = 20.0 * pairs * args.ens_steps * args.steps / (sum(ms) * 1e-3) / 1e12
+        cpu = None
+        if rank == 0 and ws == 1:
+            import oracle
+            sel = np.arange(0, args.n, max(1, args.n // 512))
+            import physgpu.dist as pdist
+            sub, body = pdist.subset_csr(off, sel)
+            cs = 20
+            t0 = time.perf_counter()
+            oracle.ensemble_run(sub, pos[body], vel[body], m[body], 1.0, args.eps, args.dt, cs,
+                                nthreads=oracle.ncpu())
+            dtc = time.perf_counter() - t0
+            cpu = {"value": len(body) * cs / dtc, "unit": "particle-steps/s",
+                   "cores": oracle.ncpu(), "kind": "port",
+                   "sample": "%d of %d systems (every %d-th), %d reference ticks each" % (
+                       len(sel), args.n, max(1, args.n // 512), cs)}
+        line = _line(args, ws, "particle-steps/s, batched ensemble of %d systems (N in [3,64]), "
+                     "FP32-comp forces, FP64 state" % args.n, value, "particle-steps/s",
+                     t / args.steps, "f32c",
+                     {"workload": "ensemble_%d_systems" % args.n, "bodies": nb,
+                      "steps_per_bench_step": args.ens_steps, "eps": args.eps, "dt": args.dt,
+                      "group": best, "autotune_ms": tune,
+                      "launch": "one persistent launch per run, captured in a CUDA graph",
+                      "l2": "state (%.1f MB) stays on chip for a whole run" % (nb * 80 / 1e6)},
+                     interactions_per_s=pairs * args.ens_steps * args.steps / (sum(ms) * 1e-3),
+                     roofline={"kernel": "ensemble_kernel<%d>" % best, "bound": "fp32",
+                               "achieved": ach, "peak": max(fp32_tf, fp32x2_tf),
+                               "unit": "TFLOP/s", "frac": ach / max(fp32_tf, fp32x2_tf),
+                               "flops_per_interaction": 20, "traffic": None},
+                     cpu_baseline=cpu, clocks=clk,
+                     gpu_launches=ctx.timings()["launches"] - l0)
+    elif args.workload == "direct":
+        pos, vel, m = ics.plummer(args.n, seed=rank)
+        out = {}
+        for name, prec in (("f64_exact", F64_EXACT), ("f64", F64), ("f32c", F32C)):
+            p = make_params(1.0, args.eps, method=DIRECT, precision=prec)
+
+            def run100():
+                ctx.upload(pos, vel, m)
+                ctx.verlet_steps(p, args.dt, 100)
+            for _ in range(args.warmup):
+                run100()
+            barrier()
+            clocks.start()
+            ms = timed(run100, args.steps)
+            clk = clocks.stop()
+            out[name] = (dist.max_over_ranks(sum(ms), device="cuda"), clk)
+        t, clk = out["f64_exact"]
+        n = args.n
+        value = ws * n * 100 * args.steps / (t * 1e-3)
+        cpu = None
+        if rank == 0 and ws == 1:
+            import oracle
+            t0 = time.perf_counter()
+            oracle.vv_run(pos, vel, m, 1.0, args.eps, args.dt, 10, method="direct")
+            dtc = (time.perf_counter() - t0) / 10
+            cpu = {"value": n / dtc, "unit": "particle-steps/s", "cores": 1, "kind": "port",
+                   "sample": "10 reference ticks (2 direct-sum evaluations each; 1024 targets "
+                             "run as one rayon task, so one core)"}
+        line = _line(args, ws, "particle-steps/s, %d-body Plummer direct sum f64, 100 VV steps"
+                     % n, value, "particle-steps/s", t / args.steps, "f64",
+                     {"workload": "direct_plummer_n%d_100_steps" % n, "eps": args.eps,
+                      "dt": args.dt, "precision": "f64_exact (bit-identical to the reference)",
+                      "bench_step": "upload + 100 Velocity-Verlet ticks on the device"},
+                     variants_ms_per_step={k: v[0] / args.steps for k, v in out.items()},
+                     cpu_baseline=cpu, clocks=clk)
+    elif args.workload == "adjoint":
+        n, nsteps = args.n, 1000
+        pos, vel, m = ics.plummer(n, seed=rank)
+        p = make_params(1.0, args.eps, precision=F64)
+        rng = np.random.default_rng(rank + 100)
+        ctx.upload(pos, vel + rng.normal(0.0, 0.01, vel.shape), m)
+        _, targets = ctx.trajectory_loss(p, args.dt, nsteps, np.zeros((n, 3)), final=True)
+        ctx.upload(pos, vel, m)
+        for _ in range(args.warmup):
+            ctx.adjoint(p, args.dt, nsteps, targets, checkpoint=32)
+        barrier()
+        clocks.start()
+        ms = timed(lambda: ctx.adjoint(p, args.dt, nsteps, targets, checkpoint=32), args.steps)
+        clk = clocks.stop()
+        t = dist.max_over_ranks(sum(ms), device="cuda")
+        value = ws * args.steps / (t * 1e-3)
+        line = _line(args, ws, "trajectory gradients/s, %d-body Plummer, 1000 VV steps, f64 "
+                     "adjoint with checkpoint 32" % n, value, "gradients/s", t / args.steps, "f64",
+                     {"workload": "adjoint_plummer_n%d_1000_steps" % n, "eps": args.eps,
+                      "dt": args.dt, "checkpoint": 32,
+                      "work_per_gradient": "2001 force evaluations + 1001 Jacobian-vector "
+                                           "products of the direct sum"},
+                     particle_steps_per_s=ws * n * nsteps * args.steps / (t * 1e-3),
+                     cpu_baseline=None, clocks=clk,
+                     note="the reference has no differentiation: no CPU baseline")
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_reference_other(args, ws, rank):
+    import oracle
+    oracle.lib()
+    if rank != 0:
+        return 0
+    import physgpu.ics as ics
+    if args.workload == "adjoint":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the reference has no differentiation of trajectories"}), flush=True)
+        return 0
+    ticks = []
+    if args.workload == "ensemble":
+        import physgpu.dist as pdist
+        off, pos, vel, m = ics.ensemble(args.n, seed=0)
+        sel = np.arange(0, args.n, max(1, args.n // 512))
+        sub, body = pdist.subset_csr(off, sel)
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            oracle.ensemble_run(sub, pos[body], vel[body], m[body], 1.0, args.eps, args.dt, 20)
+            if k >= args.warmup:
+                ticks.append((time.perf_counter() - t0) / 20)
+        value = len(body) / (sum(ticks) / len(ticks))
+        sample = "%d of %d systems, 20 ticks per step" % (len(sel), args.n)
+    else:
+        pos, vel, m = ics.plummer(args.n, seed=0)
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            oracle.vv_run(pos, vel, m, 1.0, args.eps, args.dt, 10, method="direct")
+            if k >= args.warmup:
+                ticks.append((time.perf_counter() - t0) / 10)
+        value = args.n / (sum(ticks) / len(ticks))
+        sample = "10 reference ticks per step"
+    line = {"impl": "reference", "metric": args.workload, "value": value,
+            "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sum(ticks) / len(ticks),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": args.workload, "n": args.n},
+            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": oracle.ncpu(),
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
     if args.impl == "reference":
-        return run_reference(args, ws, rank)
-    return run_ours(args, ws, rank, local)
+        if args.workload in ("bh", "galaxy"):
+            return run_reference(args, ws, rank)
+        return run_reference_other(args, ws, rank)
+    if args.workload in ("bh", "galaxy"):
+        return run_ours(args, ws, rank, local)
+    return run_other(args, ws, rank, local)
 
 
 if __name__ == "__main__":

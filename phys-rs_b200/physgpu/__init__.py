@@ -488,10 +488,10 @@ def reset_forces(world):
     world.force[:] = 0.0
 
 
-def _state_to_ctx(world, ctx, config=None):
-    ctx.upload_sectors(world.sector, world.local,
-                       config.sector_size if config else 1e12, world.mass,
-                       vel=world.velocity)
+def _state_to_ctx(world, ctx):
+    # The integrators update LocalPosition itself (integrators.rs:80): local
+    # coordinates go to the device unflattened.
+    ctx.upload(world.local, world.velocity, world.mass)
     ctx.write_component(COMP_ACCELERATION, world.acceleration)
     ctx.write_component(COMP_PREV_ACCELERATION, world.prev_acceleration)
 
