@@ -48,6 +48,8 @@ def parse():
                          "adjoint: 4096-body trajectory gradient")
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--leaf-cap", type=int, default=8)
+    ap.add_argument("--walk", default="body", choices=["body", "group"],
+                    help="Barnes-Hut walk: per body (the reference's) or per 64-body group")
     ap.add_argument("--theta", type=float, default=None)
     ap.add_argument("--eps", type=float, default=None)
     ap.add_argument("--dt", type=float, default=None)
@@ -182,11 +184,13 @@ def run_reference(args, ws, rank):
     return 0
 
 
-def workload_config(args, precision, leaf_cap):
+def workload_config(args, precision, leaf_cap, walk="body"):
     galaxy = args.workload == "galaxy"
     return {"workload": ("barnes_hut_galaxy_n%d" if galaxy else "barnes_hut_plummer_n%d") % args.n,
             "n": args.n, "theta": args.theta, "eps": args.eps, "G": 1.0, "dt": args.dt,
             "leaf_cap": leaf_cap, "precision": precision,
+            "walk": ("per body (the reference's criterion per target)" if walk == "body" else
+                     "per 64-body group (criterion at the group box's nearest point)"),
             "ics": ("30% exponential disk (R_d=1, sech^2 z0=0.1) + 70% NFW halo (r_s=3, cut 30), "
                     "seed=rank" if galaxy else "Plummer a=1, equal masses 1/N, seed=rank"),
             "l2": "flushed between timed steps (256 MiB write)"}
@@ -199,7 +203,8 @@ WALK_TRAFFIC_BYTES = 157.05e6
 
 
 def walk_traffic(args):
-    if (args.workload, args.n, args.theta, args.leaf_cap) == ("bh", 1 << 20, 0.5, 8):
+    if (args.workload, args.n, args.theta, args.leaf_cap, args.walk) == (
+            "bh", 1 << 20, 0.5, 8, "body"):
         return WALK_TRAFFIC_BYTES
     return None
 
@@ -227,8 +232,9 @@ def run_ours(args, ws, rank, local):
     else:
         pos, vel, m = ics.plummer(args.n, seed=rank)
     n = args.n
-    p32 = make_params(1.0, args.eps, args.theta, BARNES_HUT, F32C, args.leaf_cap)
-    p64 = make_params(1.0, args.eps, args.theta, BARNES_HUT, F64, args.leaf_cap)
+    flags = physgpu.GROUP_WALK if args.walk == "group" else 0
+    p32 = make_params(1.0, args.eps, args.theta, BARNES_HUT, F32C, args.leaf_cap, flags)
+    p64 = make_params(1.0, args.eps, args.theta, BARNES_HUT, F64, args.leaf_cap, flags)
 
     def barrier():
         torch.cuda.synchronize()
@@ -351,12 +357,31 @@ def run_ours(args, ws, rank, local):
             extras["accel_err_%s_vs_f64_direct_subsample" % name] = {
                 "median": float(np.median(e)), "p99": float(np.quantile(e, 0.99)),
                 "max": float(e.max()), "targets": int(len(sub))}
-        pcap1 = make_params(1.0, args.eps, args.theta, BARNES_HUT, F32C, 1)
+        pcap1 = make_params(1.0, args.eps, args.theta, BARNES_HUT, F32C, 1, flags)
         ctx.upload(pos, vel, m)
         for _ in range(2):
             ctx.verlet_steps(pcap1, args.dt, 1)
         c1, _, _ = timed_steps(pcap1, max(2, args.steps // 2))
         extras["leaf_cap1_ms_per_step"] = c1 / max(2, args.steps // 2)
+        # ---- the other walk (per body <-> per group), F32C and F64 ----
+        other = "body" if args.walk == "group" else "group"
+        oflags = physgpu.GROUP_WALK if other == "group" else 0
+        for prec, name in ((F32C, "f32c"), (F64, "fp64")):
+            po = make_params(1.0, args.eps, args.theta, BARNES_HUT, prec, args.leaf_cap, oflags)
+            ctx.upload(pos, vel, m)
+            for _ in range(2):
+                ctx.verlet_steps(po, args.dt, 1)
+            ko = max(2, args.steps // 2)
+            to, wo, io = timed_steps(po, ko)
+            extras["%s_walk_%s_ms_per_step" % (other, name)] = to / ko
+            extras["%s_walk_%s_walk_ms" % (other, name)] = statistics.median(wo)
+            extras["%s_walk_%s_interactions" % (other, name)] = statistics.median(io)
+            if prec == F32C:
+                ao = ctx.gravity_accel(po)
+                e = np.linalg.norm(ao[sub] - ad, axis=1) / np.linalg.norm(ad, axis=1)
+                extras["accel_err_%s_walk_f32c_vs_f64_direct_subsample" % other] = {
+                    "median": float(np.median(e)), "p99": float(np.quantile(e, 0.99)),
+                    "max": float(e.max())}
 
     # ---- roofline of the dominant kernel (the walk) ----
     fp32_tf, fp32x2_tf, fp64_tf = ctx.probe_peaks()
@@ -364,7 +389,8 @@ def run_ours(args, ws, rank, local):
     walk_med = statistics.median(walk_ms)
     inter_med = statistics.median(inter)
     achieved = FLOPS_PER_INTERACTION * inter_med / (walk_med * 1e-3) / 1e12
-    roof = {"kernel": "walk2_kernel (f32c)", "bound": "fp32", "achieved": achieved,
+    roof = {"kernel": ("gwalk_kernel<true> (f32c group walk)" if args.walk == "group"
+                       else "walk2_kernel (f32c)"), "bound": "fp32", "achieved": achieved,
             "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
             "peak_source": ("measured live: max of FFMA and packed FFMA2 loops on all SMs "
                             "(FMA = 2 flops); ffma %.1f, ffma2 %.1f" % (fp32_tf, fp32x2_tf)),
@@ -397,7 +423,7 @@ def run_ours(args, ws, rank, local):
             "data": "synthetic (seeded %s; no dataset)" % (
                 "Plummer sphere" if args.workload == "bh" else "exponential disk + NFW halo"),
             "config": workload_config(args, "f32c (f32 pair terms, two-sum, f64 state)",
-                                      args.leaf_cap),
+                                      args.leaf_cap, args.walk),
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "clocks": clk, "roofline": roof, "cpu_baseline": cpu,

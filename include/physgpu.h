@@ -52,6 +52,18 @@ extern "C" {
 #define PHYS_F32C 2           /* f32 pair terms on double-float relative coordinates,
                                  two-sum compensated f32 accumulation, f64 state     */
 
+/* Barnes-Hut walk per group of 64 key-adjacent bodies (PHYS_F64 and
+ * PHYS_F32C only): a cell is taken as a monopole only when the reference's
+ * criterion (2h)^2 < theta^2 d^2 holds for the nearest point of the group's
+ * bounding box (so for every body of the group); the accepted cells and the
+ * bodies of opened leaves form one interaction list that the whole group
+ * evaluates, and pairs inside the group are exact.  No cell is taken as a
+ * monopole that the per-body criterion would open, and every pair the
+ * per-body walk takes exactly stays exact; the walk order and the sums are
+ * not the reference's.  No counterpart in the reference
+ * (gravity_tree.rs:171-209 walks per body). */
+#define PHYS_FLAG_GROUP_WALK 1
+
 typedef struct phys_ctx phys_ctx;
 
 /* UniverseConfig (src/core/config.rs:26-59) fields the gravity path reads,
@@ -65,7 +77,7 @@ typedef struct phys_params {
   int32_t leaf_cap;   /* BH leaf capacity: 1 = the reference octree; 2..16 =
                          bucket leaves (criterion on the cell, exact pairs when
                          opened).  F64_EXACT requires 1.                      */
-  int32_t flags;      /* reserved, must be 0                                  */
+  int32_t flags;      /* 0, or PHYS_FLAG_GROUP_WALK                          */
 } phys_params;
 
 /* Per-call device timings of the last force evaluation / step (CUDA events

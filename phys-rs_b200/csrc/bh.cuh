@@ -52,6 +52,24 @@ struct __align__(16) Rec32x2 {
 struct __align__(16) Body32x2 {
   float4 q0, q1, q2, q3;  // same layout, ropen2 slot unused
 };
+// Group-walk record, breadth-first order (children of a cell contiguous).
+// l = {a, (b << 2) | type, first body, end body} (sorted positions; the
+// cell holds bodies [first, end)).  internal: a = first child, b = child
+// count; one-body leaf: a = the body it stands for (the last inserted one for
+// a guard leaf of capacity 1); bucket leaf: a = first body, b = body count;
+// skip: a cell whose total mass is not > 0 (never the root).
+constexpr int kGroupMax = 64;  // bodies per target group (one warp, two per lane)
+constexpr int kGInternal = 0;
+constexpr int kGSingle = 1;
+constexpr int kGBucket = 2;
+constexpr int kGSkip = 3;
+struct __align__(16) GNode {
+  float4 hi;    // x_hi, y_hi, z_hi, mass (f32)
+  float4 lo;    // x_lo, y_lo, z_lo, cell side squared (2h)^2 (f32)
+  int4 l;
+  double4 c64;  // x, y, z, mass (f64)
+};
+static_assert(sizeof(GNode) == 80, "GNode layout");
 struct __align__(16) Rec64 {
   double4 a;  // x, y, z, mass
   int4 l;
@@ -73,13 +91,20 @@ struct BhTree {
   const float4* body_hi = nullptr;    // sorted bodies, double-float hi + f32 mass
   const float4* body_lo = nullptr;
   const TreeHeader* hdr = nullptr;
+  const GNode* gnode = nullptr;       // group-walk records (breadth-first)
+  const int2* groups = nullptr;       // group-walk target groups: body ranges [x, y),
+                                      // room for n more (re-queued subgroups) after n
+  const int32_t* ngroups = nullptr;   // device: number of groups
+  int32_t* group_ctr = nullptr;       // device: 3 walk counters (reset per walk)
   const uint64_t* keys_hi_sorted = nullptr;  // descent keys, octants 0..20, sorted
   const uint64_t* keys_lo = nullptr;         // octants 21..39, caller order
 };
 
 // tree.cu
-int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t);
+int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool need_group = false);
 // walk.cu
+int bh_group_walk(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force,
+                  double* ox, double* oy, double* oz);
 int bh_walk(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force, double* ox,
             double* oy, double* oz);
 

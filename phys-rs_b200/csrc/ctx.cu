@@ -141,14 +141,17 @@ int check_params(phys_ctx* c, const phys_params* p) {
     return fail(c, PHYS_ERR_ARG, "leaf_cap %d outside 1..%d", p->leaf_cap, kMaxLeafCap);
   if (p->method == PHYS_BARNES_HUT && p->precision == PHYS_F64_EXACT && p->leaf_cap != 1)
     return fail(c, PHYS_ERR_ARG, "F64_EXACT Barnes-Hut follows the reference octree: leaf_cap 1");
-  if (p->flags != 0) return fail(c, PHYS_ERR_ARG, "flags must be 0");
+  if (p->flags & ~PHYS_FLAG_GROUP_WALK) return fail(c, PHYS_ERR_ARG, "unknown flags 0x%x", p->flags);
+  if ((p->flags & PHYS_FLAG_GROUP_WALK) &&
+      (p->method != PHYS_BARNES_HUT || p->precision == PHYS_F64_EXACT))
+    return fail(c, PHYS_ERR_ARG, "the group walk is Barnes-Hut with PHYS_F64 or PHYS_F32C");
   if (!(p->theta >= 0.0)) return fail(c, PHYS_ERR_ARG, "theta must be >= 0");
   return PHYS_OK;
 }
 
 bool same_params(const phys_params& a, const phys_params& b) {
   return a.G == b.G && a.eps == b.eps && a.theta == b.theta && a.method == b.method &&
-         a.precision == b.precision && a.leaf_cap == b.leaf_cap;
+         a.precision == b.precision && a.leaf_cap == b.leaf_cap && a.flags == b.flags;
 }
 
 // One force evaluation on the device: accelerations into c->ax.. (want_force

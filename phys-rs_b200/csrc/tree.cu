@@ -589,11 +589,126 @@ finalize_kernel(int64_t nnodes, int4* __restrict__ link, double4* __restrict__ m
   }
 }
 
+// Breadth-first order: node ids stably sorted by depth (one radix pass on
+// pre-order input); inverse map.
+__global__ void depth_key_kernel(int64_t nnodes, const int4* __restrict__ link,
+                                 uint64_t* __restrict__ key, uint32_t* __restrict__ val) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnodes;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    key[k] = (uint64_t)(link[k].w & kMetaDepth);
+    val[k] = (uint32_t)k;
+  }
+}
+
+__global__ void invert_kernel(int64_t nnodes, const uint32_t* __restrict__ bfs2pre,
+                              int32_t* __restrict__ pre2bfs) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nnodes;
+       j += (int64_t)gridDim.x * blockDim.x)
+    pre2bfs[bfs2pre[j]] = (int32_t)j;
+}
+
+__global__ void __launch_bounds__(kBlock)
+gnode_kernel(int64_t nnodes, const uint32_t* __restrict__ bfs2pre,
+             const int32_t* __restrict__ pre2bfs, const int4* __restrict__ link,
+             const double4* __restrict__ mc, const int32_t* __restrict__ nchild, int leaf_cap,
+             const double4* __restrict__ body64, const TreeHeader* __restrict__ hdr,
+             GNode* __restrict__ g) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nnodes;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)bfs2pre[j];
+    const int4 lk = link[k];
+    const int d = lk.w & kMetaDepth;
+    const int cntb = lk.z - lk.y;
+    const bool leaf = lk.w & kMetaLeaf;
+    double4 r = mc[k];
+    int4 l;
+    if (!(lk.w & kMetaGate) && k != 0) {
+      l = make_int4(0, kGSkip, lk.y, lk.z);
+    } else if (leaf && (cntb == 1 || ((lk.w & kMetaGuard) && leaf_cap == 1))) {
+      const int self = cntb == 1 ? lk.y : lk.z - 1;  // guard leaf: last inserted body
+      r = body64[self];
+      l = make_int4(self, (1 << 2) | kGSingle, lk.y, lk.z);
+    } else if (leaf) {
+      l = make_int4(lk.y, (cntb << 2) | kGBucket, lk.y, lk.z);
+    } else {
+      // children of a pre-order cell start at k + 1
+      l = make_int4(pre2bfs[k + 1], (nchild[k] << 2) | kGInternal, lk.y, lk.z);
+    }
+    GNode o;
+    split_df(r.x, o.hi.x, o.lo.x);
+    split_df(r.y, o.hi.y, o.lo.y);
+    split_df(r.z, o.hi.z, o.lo.z);
+    o.hi.w = (float)r.w;
+    o.lo.w = (float)hdr->s2[d];
+    o.l = l;
+    o.c64 = r;
+    g[j] = o;
+  }
+}
+
+// Target groups of the group walk: every cell with more than kGroupMax
+// bodies splits its children into runs of consecutive children with at most
+// kGroupMax bodies between them (a child with more starts its own groups);
+// a leaf with more (guard depth) is cut into chunks; a root with at most
+// kGroupMax bodies is one group.  The groups partition the bodies into
+// key-contiguous ranges that each lie inside one cell.  Cells are taken in
+// breadth-first order, so the groups of large shallow cells (the sparse
+// outskirts, whose walks are the longest) come first and the walk's dynamic
+// scheduling starts them early.  Pass 1 counts per cell (cnt, indexed by
+// breadth-first position j, cnt[nnodes] = 0 for the scan), pass 2 writes the
+// ranges from the scanned offsets.
+template <bool kEmit>
+__global__ void group_kernel(int64_t nnodes, const uint32_t* __restrict__ bfs2pre,
+                             const int4* __restrict__ link, const int32_t* __restrict__ nchild,
+                             int32_t* __restrict__ cnt, const int32_t* __restrict__ off,
+                             int2* __restrict__ out, int64_t cap) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j <= nnodes;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    if (j == nnodes) {
+      if (!kEmit) cnt[j] = 0;
+      continue;
+    }
+    const int64_t k = bfs2pre[j];
+    const int4 lk = link[k];
+    const int ck = lk.z - lk.y;
+    int r = 0;
+    auto put = [&](int b0, int b1) {
+      if (kEmit && off[j] + r < cap) out[off[j] + r] = make_int2(b0, b1);
+      ++r;
+    };
+    if (ck <= kGroupMax) {
+      if (k == 0) put(lk.y, lk.z);
+    } else if (lk.w & kMetaLeaf) {
+      for (int b = lk.y; b < lk.z; b += kGroupMax) put(b, min(b + kGroupMax, lk.z));
+    } else {
+      int c = (int)k + 1, rb = -1, re = -1;
+      const int nc = nchild[k];
+      for (int i = 0; i < nc && c < nnodes; ++i) {
+        const int4 lc = link[c];
+        const int cc = lc.z - lc.y;
+        if (cc > kGroupMax) {
+          if (rb >= 0) put(rb, re);
+          rb = -1;
+        } else if (rb >= 0 && re - rb + cc <= kGroupMax) {
+          re = lc.z;
+        } else {
+          if (rb >= 0) put(rb, re);
+          rb = lc.y;
+          re = lc.z;
+        }
+        c = lc.x;
+      }
+      if (rb >= 0) put(rb, re);
+    }
+    if (!kEmit) cnt[j] = r;
+  }
+}
+
 }  // namespace
 
 // Builds the tree for the current positions.  One host synchronisation reads
 // the node count (two with bucket leaves).
-int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t) {
+int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool need_group) {
   const int64_t n = c->n;
   const bool exact = p->precision == PHYS_F64_EXACT;
   uint64_t* khi = nullptr;
@@ -740,10 +855,45 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t) {
     PHYS_TRY(ws_alloc(c, WS_NODE_HI, nnodes, &w32x2));
   else if (need_f32)
     PHYS_TRY(ws_alloc(c, WS_NODE_HI, nnodes, &w32));
-  else if (!exact)
+  else if (!exact && !need_group)
     PHYS_TRY(ws_alloc(c, WS_NODE_LO, nnodes, &w64));
   PHYS_LAUNCH(c, finalize_kernel, grid_for(nnodes), kBlock, 0, nnodes, link, mc, exact ? 0 : 1,
               p->leaf_cap, body64, c->d_hdr, rec64, w32, w64, w32x2);
+  if (need_group) {
+    // breadth-first records for the group walk
+    uint64_t *dk = nullptr, *dk_alt = nullptr;
+    uint32_t *dv = nullptr, *dv_alt = nullptr;
+    int32_t* pre2bfs = nullptr;
+    GNode* g = nullptr;
+    PHYS_TRY(ws_alloc(c, WS_ENTRIES, nnodes, &dk));
+    PHYS_TRY(ws_alloc(c, WS_ENTRIES_ALT, nnodes, &dk_alt));
+    PHYS_TRY(ws_alloc(c, WS_KEEP, nnodes, &dv));
+    PHYS_TRY(ws_alloc(c, WS_NEWID, nnodes, &dv_alt));
+    PHYS_TRY(ws_alloc(c, WS_EOFF, nnodes + 1, &pre2bfs));
+    PHYS_TRY(ws_alloc(c, WS_ENS5, nnodes, &g));
+    PHYS_LAUNCH(c, depth_key_kernel, grid_for(nnodes), kBlock, 0, nnodes, link, dk, dv);
+    bool alt = false;
+    PHYS_TRY(radix_sort_u64(c, dk, dv, dk_alt, dv_alt, nnodes, 0, 8, &alt));
+    const uint32_t* bfs2pre = alt ? dv_alt : dv;
+    PHYS_LAUNCH(c, invert_kernel, grid_for(nnodes), kBlock, 0, nnodes, bfs2pre, pre2bfs);
+    PHYS_LAUNCH(c, gnode_kernel, grid_for(nnodes), kBlock, 0, nnodes, bfs2pre, pre2bfs, link, mc,
+                nchild, p->leaf_cap, body64, c->d_hdr, g);
+    t->gnode = g;
+    int32_t *gcnt = nullptr, *goff = nullptr, *gctr = nullptr;
+    int2* groups = nullptr;
+    PHYS_TRY(ws_alloc(c, WS_NCOUNT, nnodes + 1, &gcnt));
+    PHYS_TRY(ws_alloc(c, WS_GROUP_OFF, nnodes + 1, &goff));
+    PHYS_TRY(ws_alloc(c, WS_GROUPS, 2 * n, &groups));  // groups, then re-queued subgroups
+    PHYS_TRY(ws_alloc(c, WS_GROUP_CTR, 3, &gctr));
+    PHYS_LAUNCH(c, group_kernel<false>, grid_for(nnodes + 1), kBlock, 0, nnodes, bfs2pre, link,
+                nchild, gcnt, goff, groups, n);
+    PHYS_TRY(scan_exclusive_i32(c, gcnt, goff, nnodes + 1));
+    PHYS_LAUNCH(c, group_kernel<true>, grid_for(nnodes + 1), kBlock, 0, nnodes, bfs2pre, link,
+                nchild, gcnt, goff, groups, n);
+    t->groups = groups;
+    t->ngroups = goff + nnodes;
+    t->group_ctr = gctr;
+  }
   t->n = n;
   t->nnodes = nnodes;
   t->leaf_cap = p->leaf_cap;
@@ -769,7 +919,8 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t) {
 int bh_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, double* oy,
             double* oz) {
   BhTree t;
-  PHYS_TRY(bh_build(c, p, p->precision == PHYS_F32C, &t));
+  const bool group = (p->flags & PHYS_FLAG_GROUP_WALK) != 0;
+  PHYS_TRY(bh_build(c, p, p->precision == PHYS_F32C && !group, &t, group));
   return bh_walk(c, p, t, want_force, ox, oy, oz);
 }
 

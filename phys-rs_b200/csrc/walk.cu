@@ -480,7 +480,9 @@ int bh_walk(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force,
   const int grid = (int)ceil_div(n, kWalkBlock);
   PHYS_CUDA(c, cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned long long), c->stream));
   PHYS_CUDA(c, cudaEventRecord(c->ev[6], c->stream));
-  if (p->precision == PHYS_F64_EXACT) {
+  if (p->flags & PHYS_FLAG_GROUP_WALK) {
+    PHYS_TRY(bh_group_walk(c, p, t, want_force, ox, oy, oz));
+  } else if (p->precision == PHYS_F64_EXACT) {
     PHYS_LAUNCH(c, walk_exact_kernel, grid, kWalkBlock, 0, n, t.nnodes, t.link, t.rec64, t.body64,
                 t.perm, t.hdr, p->G, eps2, (int)want_force, ox, oy, oz, c->d_counter, c->d_status);
   } else if (p->precision == PHYS_F64) {

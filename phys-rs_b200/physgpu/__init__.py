@@ -26,6 +26,7 @@ LIB_PATH = os.path.join(_PKG, "lib", "libphysgpu.so")
 OK, ERR_ARG, ERR_CUDA, ERR_OOM, ERR_NONFINITE, ERR_TIMEOUT, ERR_STATE = range(7)
 DIRECT, BARNES_HUT = 0, 1
 F64_EXACT, F64, F32C = 0, 1, 2
+GROUP_WALK = 1  # phys_params.flags: Barnes-Hut walk per group of 64 bodies
 COMP_POSITION, COMP_VELOCITY, COMP_ACCELERATION, COMP_PREV_ACCELERATION, COMP_MASS = range(5)
 
 PRECISIONS = {"f64_exact": F64_EXACT, "f64": F64, "f32c": F32C}
@@ -137,10 +138,11 @@ def _col(a, k):
     return np.ascontiguousarray(a[:, k], dtype=np.float64)
 
 
-def make_params(G, eps, theta=0.5, method=DIRECT, precision=F64_EXACT, leaf_cap=1):
+def make_params(G, eps, theta=0.5, method=DIRECT, precision=F64_EXACT, leaf_cap=1, flags=0):
     if isinstance(precision, str):
         precision = PRECISIONS[precision]
-    return Params(float(G), float(eps), float(theta), int(method), int(precision), int(leaf_cap), 0)
+    return Params(float(G), float(eps), float(theta), int(method), int(precision), int(leaf_cap),
+                  int(flags))
 
 
 class Context:
