@@ -95,7 +95,7 @@ struct BhTree {
   const int2* groups = nullptr;       // group-walk target groups: body ranges [x, y),
                                       // room for n more (re-queued subgroups) after n
   const int32_t* ngroups = nullptr;   // device: number of groups
-  int32_t* group_ctr = nullptr;       // device: 3 walk counters (reset per walk)
+  int32_t* group_ctr = nullptr;       // device: walk counters (reset per walk)
   const uint64_t* keys_hi_sorted = nullptr;  // descent keys, octants 0..20, sorted
   const uint64_t* keys_lo = nullptr;         // octants 21..39, caller order
 };

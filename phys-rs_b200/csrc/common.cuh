@@ -112,7 +112,7 @@ enum WsSlot {
   WS_ENTRIES, WS_ENTRIES_ALT, WS_EOFF,
   WS_DIRECT_PART, WS_ADJ0, WS_ADJ1, WS_ADJ2, WS_ADJ3, WS_ADJ4,
   WS_ENS0, WS_ENS1, WS_ENS2, WS_ENS3, WS_ENS4, WS_ENS5, WS_ENS6, WS_ENS7,
-  WS_GROUPS, WS_GROUP_OFF, WS_GROUP_CTR,
+  WS_GROUPS, WS_GROUP_OFF, WS_GROUP_CTR, WS_GROUP_POOL, WS_GROUP_ITEMS,
   WS_COUNT_
 };
 

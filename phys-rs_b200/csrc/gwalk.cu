@@ -5,24 +5,30 @@
 // criterion (2h)^2 < theta^2 d^2 at :194).  Here the bodies are split into
 // groups that each lie inside one cell (the children of a cell with more
 // than 64 bodies, consecutive small siblings packed together; built with the
-// tree), a warp takes groups from a global counter, bounds each with a box,
-// and walks the tree once for all its bodies:
-//   - the warp pops up to 32 cells from a stack in shared memory, one per
-//     lane, and tests each against the box: a cell is a monopole only when
-//     (2h)^2 < theta^2 d_min^2, d_min the distance from its centre of mass to
-//     the nearest point of the box (d_min <= d for every target, so the
-//     per-body criterion holds for each of them);
+// tree), and the tree is walked once per group:
+//   - a warp pops up to 32 cells from a stack in shared memory, one per
+//     lane, and tests each against the group's bounding box: a cell is a
+//     monopole only when (2h)^2 < theta^2 d_min^2, d_min the distance from
+//     its centre of mass to the nearest point of the box (d_min <= d for
+//     every target, so the per-body criterion holds for each of them);
 //   - an opened cell pushes its children (contiguous in the breadth-first
 //     record array); a one-body leaf, an accepted cell and every body of an
-//     opened bucket leaf become entries of the interaction list, spread over
-//     the lanes (each lane writes consecutive slots);
+//     opened bucket leaf become entries of the group's interaction list;
 //   - the group's own bodies never enter the list: a cell whose bodies all
 //     belong to the group is skipped, one that holds some of them is always
 //     opened, and pairs inside the group are summed exactly in a separate
-//     pass that skips i == j;
-//   - a full list is evaluated by all targets at once: lane l reads the
-//     entries as broadcast shared-memory loads and accumulates its two
-//     targets.
+//     pass that skips i == j.
+// Three launches:
+//   1. glist_kernel walks every group and writes its list as 4-byte codes
+//      (cell or body index) to a per-warp region of a global pool; a group
+//      whose list passes kGListLimit entries (a sparse group whose box
+//      reaches a much denser region) is abandoned and re-queued as
+//      subgroups of kGSplit consecutive bodies, whose lists are far shorter;
+//   2. geval_kernel evaluates the lists: per batch of kGList entries the
+//      lanes gather the sources into shared memory, then every lane
+//      accumulates its two targets over the batch (broadcast loads);
+//   3. gwalk_kernel walks and evaluates the re-queued subgroups in one pass
+//      (list in shared memory, evaluated whenever it fills).
 // The list arithmetic is the per-body walk's: F64 = f64 FMA + rsqrt on
 // absolute coordinates; F32C = f32 pair terms on double-float coordinates
 // relative to the group's first body, r = (hi_j - hi_i) + (lo_j - lo_i), two
@@ -40,35 +46,56 @@
 // tree has each cell pushed once, so a walk ends after at most nnodes pops;
 // a malformed tree (child index not after its parent, more pops than cells)
 // sets kStatOverflow and the warp stops.
+#include <algorithm>
 #include <climits>
 
 #include "bh.cuh"
 
 #ifndef GWALK_FLUSH_PAIRS
-#define GWALK_FLUSH_PAIRS 8
+#define GWALK_FLUSH_PAIRS 16
+#endif
+#ifndef GWALK_LIST_LIMIT
+#define GWALK_LIST_LIMIT 8192
+#endif
+#ifndef GWALK_SPLIT
+#define GWALK_SPLIT 4
+#endif
+#ifndef GWALK_FAR
+#define GWALK_FAR 1
+#endif
+#ifndef GWALK_POOL_PER_BODY
+#define GWALK_POOL_PER_BODY 128
 #endif
 
 namespace phys {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kGWarps = 4;
+constexpr int kGWarps = 4;  // evaluating kernels
 constexpr int kGBlock = 32 * kGWarps;
-constexpr int kGStack = 1024;   // node ids per warp
-constexpr int kGList = 256;     // list entries per warp, 32 bytes each
+constexpr int kLWarps = 8;  // list kernel
+constexpr int kLBlock = 32 * kLWarps;
+constexpr int kGStack = 1024;  // node ids per warp
+constexpr int kGList = 256;    // shared-memory list entries per warp, 32 bytes each
 constexpr int kGThrottle = kGStack - 8 - 7 * kMaxLevels;
 constexpr int kGFlushPairs = GWALK_FLUSH_PAIRS;
-constexpr int kGListLimit = 8192;  // first-pass list budget (a typical group lists ~3-4k)
-constexpr int kGSplit = 4;         // bodies per re-queued subgroup
-// per warp: stack | list | emission records (end, kind, a, olo, ohi per lane)
+constexpr int kGListLimit = GWALK_LIST_LIMIT;  // first-pass budget (typical lists: 3-4k)
+constexpr int kGSplit = GWALK_SPLIT;            // bodies per re-queued subgroup
+// fused kernel, per warp: stack | list | emission records (end, kind, a, olo,
+// ohi and the source double4 per lane)
 constexpr int kGListOff = kGStack * 4;
 constexpr int kGRecOff = kGListOff + kGList * 32;
-constexpr int kGSmemWarp = kGRecOff + 5 * 32 * 4;
+constexpr int kGSmemWarp = kGRecOff + 5 * 32 * 4 + 32 * 32;
 constexpr int kGSmem = kGWarps * kGSmemWarp;
+constexpr int kLSmem = kLWarps * kGStack * 4;  // list kernel: stacks
+// evaluation kernel, per warp: near list (7 arrays) | far list (4 arrays)
+constexpr int kESmemWarp = kGList * 7 * 4 + kGList * 4 * 4;
+constexpr int kESmem = kGWarps * kESmemWarp;
 static_assert(kGroupMax == 64, "two targets per lane");
 static_assert(kGThrottle >= 7 * 32 + 7, "stack too small for batched pops");
 static_assert(kGThrottle + 7 * kMaxLevels + 1 <= kGStack, "stack bound");
 static_assert(kGList % 4 == 0 && kGFlushPairs % 2 == 0, "list chunks of 4 entries");
+static_assert((kGRecOff + 5 * 32 * 4) % 16 == 0, "record alignment");
 
 __device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
 __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
@@ -107,73 +134,189 @@ __device__ __forceinline__ void two_sum2(float2 a, float2 b, float2& s, float2& 
   e = __fadd2_rn(__fadd2_rn(a, make_float2(-ab.x, -ab.y)), __fadd2_rn(b, make_float2(-bb.x, -bb.y)));
 }
 
-// F32C list, structure of arrays (slot-consecutive writes hit distinct banks;
-// the evaluation reads four entries per 16-byte load).
-struct List32 {
-  float *hx, *hy, *hz, *m, *lx, *ly, *lz;
+// ---------------------------------------------------------------------------
+// Group box and node classification
+// ---------------------------------------------------------------------------
+struct Box {
+  float cx, cy, cz, bx, by, bz;  // centre and half extent, relative to X0
+  float hx, lx, hy, ly, hz, lz;  // X0 as double-float
 };
 
-// Forces on the bodies [base, gend).  Returns false, with nothing written,
-// when the interaction list grows past `limit` entries.
+// Warp-collective: box of the targets ta, tb of every lane (idle lanes pass
+// X0, a group body).
+__device__ __forceinline__ Box group_box(double4 X0, double4 ta, double4 tb) {
+  Box B;
+  const float ax = (float)(ta.x - X0.x), ay = (float)(ta.y - X0.y), az = (float)(ta.z - X0.z);
+  const float bx = (float)(tb.x - X0.x), by = (float)(tb.y - X0.y), bz = (float)(tb.z - X0.z);
+  const float mnx = warp_min(fminf(ax, bx)), mxx = warp_max(fmaxf(ax, bx));
+  const float mny = warp_min(fminf(ay, by)), mxy = warp_max(fmaxf(ay, by));
+  const float mnz = warp_min(fminf(az, bz)), mxz = warp_max(fmaxf(az, bz));
+  B.cx = 0.5f * (mnx + mxx);
+  B.cy = 0.5f * (mny + mxy);
+  B.cz = 0.5f * (mnz + mxz);
+  // widened by the rounding of the f32 coordinates (a few ulp of |c| + b)
+  B.bx = 0.5f * (mxx - mnx);
+  B.by = 0.5f * (mxy - mny);
+  B.bz = 0.5f * (mxz - mnz);
+  B.bx = B.bx * (1.0f + 1e-6f) + 1e-6f * (fabsf(B.cx) + B.bx);
+  B.by = B.by * (1.0f + 1e-6f) + 1e-6f * (fabsf(B.cy) + B.by);
+  B.bz = B.bz * (1.0f + 1e-6f) + 1e-6f * (fabsf(B.cz) + B.bz);
+  split_df(X0.x, B.hx, B.lx);
+  split_df(X0.y, B.hy, B.ly);
+  split_df(X0.z, B.hz, B.lz);
+  return B;
+}
+
+// What one popped cell contributes: children to push, and list entries
+// (kind 1: the cell itself / the body of a one-body leaf, source c64 of
+// record a; kind 2: the bodies [a, a + nent) of a bucket leaf, skipping the
+// group's range [olo, ohi)).
+struct NodeOut {
+  int npush, cfirst, nent, kind, a, olo, ohi;
+  bool malformed;
+  double4 c64;
+};
+
+template <bool kNeedC64>
+__device__ __forceinline__ void classify(int nd, int base, int gend, int nnodes, const Box& B,
+                                         float theta2f, const GNode* __restrict__ gn,
+                                         NodeOut& o) {
+  o.npush = o.cfirst = o.nent = o.kind = o.a = o.olo = o.ohi = 0;
+  o.malformed = false;
+  o.c64 = make_double4(0.0, 0.0, 0.0, 0.0);
+  if (nd < 0) return;
+  // the whole record in one round trip
+  const GNode* g = gn + nd;
+  const int4 l = __ldg(&g->l);
+  const float4 h = __ldg(&g->hi), lo = __ldg(&g->lo);
+  if (kNeedC64) o.c64 = ldg_d4(&g->c64);
+  const int type = l.y & 3, cnt = l.y >> 2;
+  const bool inside = l.z >= base && l.w <= gend;  // only group bodies
+  if (type == kGSkip || inside) return;
+  if (type == kGSingle) {
+    if (l.x < base || l.x >= gend) {
+      o.nent = 1;
+      o.kind = 1;
+      o.a = nd;
+    }
+    return;
+  }
+  const bool overlap = l.z < gend && l.w > base;
+  bool acc = false;
+  if (!overlap) {
+    const float rx = (h.x - B.hx) + (lo.x - B.lx);
+    const float ry = (h.y - B.hy) + (lo.y - B.ly);
+    const float rz = (h.z - B.hz) + (lo.z - B.lz);
+    const float dx = fmaxf(fabsf(rx - B.cx) - B.bx, 0.f);
+    const float dy = fmaxf(fabsf(ry - B.cy) - B.by, 0.f);
+    const float dz = fmaxf(fabsf(rz - B.cz) - B.bz, 0.f);
+    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    acc = lo.w < theta2f * d2 * (1.0f - 1e-5f);
+  }
+  if (acc) {
+    o.nent = 1;
+    o.kind = 1;
+    o.a = nd;
+  } else if (type == kGInternal) {
+    if (l.x <= nd || cnt < 1 || cnt > 8 || l.x + cnt > nnodes) {
+      o.malformed = true;
+    } else {
+      o.npush = cnt;
+      o.cfirst = l.x;
+    }
+  } else {  // bucket leaf opened: its bodies outside the group
+    o.a = l.z;
+    o.olo = max(l.z, base);
+    o.ohi = min(l.w, gend);
+    o.nent = (l.w - l.z) - max(o.ohi - o.olo, 0);
+    o.kind = 2;
+  }
+}
+
+// Sorted position of entry j of a bucket leaf's bodies outside the group.
+__device__ __forceinline__ int bucket_body(int a, int olo, int ohi, int j) {
+  int q = a + j;
+  if (olo < ohi && q >= olo) q += ohi - olo;
+  return q;
+}
+
+// Walks the tree for the group [base, gend); sink(etot, eoff, o) receives
+// each round's entries (etot in all, this lane's at eoff) and returns false
+// to stop.  Returns 1 when the walk completed, 0 when the list passed
+// `limit` entries or the sink stopped it, -1 on a malformed tree or a full
+// stack.
+template <bool kNeedC64, class Sink>
+__device__ __forceinline__ int traverse(int lane, int base, int gend, int nnodes, int limit,
+                                        int* stk, const Box& B, float theta2f,
+                                        const GNode* __restrict__ gn, Sink& sink) {
+  int ssize = 1, listed = 0;
+  long long pops = 0;
+  if (lane == 0) stk[0] = 0;
+  __syncwarp();
+  while (ssize > 0) {
+    if (listed > limit) return 0;
+    const int k = ssize <= kGThrottle - 7 ? min(min(32, ssize), (kGThrottle - ssize) / 7) : 1;
+    const int nd = lane < k ? stk[ssize - 1 - lane] : -1;
+    ssize -= k;
+    pops += k;
+    __syncwarp();
+    NodeOut o;
+    classify<kNeedC64>(nd, base, gend, nnodes, B, theta2f, gn, o);
+    if (pops > nnodes) o.malformed = true;
+    // both scans first (independent chains), then pushes, then entries
+    const int pin = warp_incl_scan(o.npush, lane);
+    const int ein = warp_incl_scan(o.nent, lane);
+    const int ptot = __shfl_sync(kFull, pin, 31);
+    const int etot = __shfl_sync(kFull, ein, 31);
+    if (__any_sync(kFull, o.malformed) || ssize + ptot > kGStack) return -1;
+    for (int c = 0; c < o.npush; ++c) stk[ssize + pin - o.npush + c] = o.cfirst + c;
+    ssize += ptot;
+    listed += etot;
+    if (etot > 0 && !sink(etot, ein - o.nent, o)) return 0;
+    __syncwarp();  // pushes and entries visible to every lane
+  }
+  return 1;
+}
+
+// ---------------------------------------------------------------------------
+// Evaluation of a list against the group's targets
+// ---------------------------------------------------------------------------
+// The F32C list in shared memory is a structure of arrays (slot-consecutive
+// writes hit distinct banks; the evaluation reads four entries per 16-byte
+// load).
 template <bool kF32>
-__device__ __forceinline__ bool group_forces(
-    int lane, int base, int gend, int nnodes, int limit, int* stk, unsigned char* lbase, int* rec,
-    const GNode* __restrict__ gn, const double4* __restrict__ body64,
-    const uint32_t* __restrict__ perm, double G, double eps2, float theta2f, int want_force,
-    double* __restrict__ ox, double* __restrict__ oy, double* __restrict__ oz,
-    unsigned long long& ninter_out, bool& bad, int32_t* status) {
-  const int nvalid = gend - base;
-  const int ia = base + 2 * lane, ib = ia + 1;
-  const bool va = ia < gend, vb = ib < gend;
-  const double4 X0 = body64[base];
-  const double4 ta = va ? body64[ia] : X0;
-  const double4 tb = vb ? body64[ib] : X0;
-  List32 L;
-  {
-    float* f = reinterpret_cast<float*>(lbase);
-    L.hx = f;
-    L.hy = f + kGList;
-    L.hz = f + 2 * kGList;
-    L.m = f + 3 * kGList;
-    L.lx = f + 4 * kGList;
-    L.ly = f + 5 * kGList;
-    L.lz = f + 6 * kGList;
-  }
-  double4* lst64 = reinterpret_cast<double4*>(lbase);
-  int* r_end = rec;
-  int* r_kind = rec + 32;
-  int* r_a = rec + 64;
-  int* r_olo = rec + 96;
-  int* r_ohi = rec + 128;
-
-  // group box in f32, relative to X0 (idle lanes sit at X0, a group body)
-  float cx, cy, cz, bx, by, bz;
-  {
-    const float ax_ = (float)(ta.x - X0.x), ay_ = (float)(ta.y - X0.y), az_ = (float)(ta.z - X0.z);
-    const float bx_ = (float)(tb.x - X0.x), by_ = (float)(tb.y - X0.y), bz_ = (float)(tb.z - X0.z);
-    const float mnx = warp_min(fminf(ax_, bx_)), mxx = warp_max(fmaxf(ax_, bx_));
-    const float mny = warp_min(fminf(ay_, by_)), mxy = warp_max(fmaxf(ay_, by_));
-    const float mnz = warp_min(fminf(az_, bz_)), mxz = warp_max(fmaxf(az_, bz_));
-    cx = 0.5f * (mnx + mxx);
-    cy = 0.5f * (mny + mxy);
-    cz = 0.5f * (mnz + mxz);
-    // widen by the rounding of the f32 coordinates (a few ulp of |c| + b)
-    bx = 0.5f * (mxx - mnx);
-    by = 0.5f * (mxy - mny);
-    bz = 0.5f * (mxz - mnz);
-    bx = bx * (1.0f + 1e-6f) + 1e-6f * (fabsf(cx) + bx);
-    by = by * (1.0f + 1e-6f) + 1e-6f * (fabsf(cy) + by);
-    bz = bz * (1.0f + 1e-6f) + 1e-6f * (fabsf(cz) + bz);
-  }
-  float x0hx, x0lx, x0hy, x0ly, x0hz, x0lz;
-  split_df(X0.x, x0hx, x0lx);
-  split_df(X0.y, x0hy, x0ly);
-  split_df(X0.z, x0hz, x0lz);
-
-  // F32C target state: negated double-float offsets from X0, duplicated for
-  // packed operands (both halves = the same target)
+struct Evaluator {
+  int lane, nvalid, ia, ib;
+  bool va, vb;
+  bool two;  // two targets per lane (more than 32 bodies), else one
+  double4 X0, ta, tb;
+  double eps2;
+  float* f;        // F32C list: hx, hy, hz, m, lx, ly, lz arrays of kGList
+  float* ff;       // F32C far list: hx, hy, hz, m arrays of kGList (or null)
+  double4* lst64;  // F64 list
   float2 nhxa, nhya, nhza, nlxa, nlya, nlza, nhxb, nhyb, nhzb, nlxb, nlyb, nlzb;
-  {
+  float2 e2;
+  float2 pxa, pya, pza, pxb, pyb, pzb;  // partials (entry halves)
+  float2 Hx, Hy, Hz, Lx, Ly, Lz;        // (target a, target b)
+  double ax, ay, az, bx, by, bz;        // F64 sums
+
+  __device__ __forceinline__ void init(int lane_, int base, int gend,
+                                       const double4* __restrict__ body64, unsigned char* lbase,
+                                       double eps2_) {
+    lane = lane_;
+    nvalid = gend - base;
+    two = nvalid > 32;
+    ia = two ? base + 2 * lane : base + lane;
+    ib = two ? ia + 1 : gend;
+    va = ia < gend;
+    vb = ib < gend;
+    X0 = body64[base];
+    ta = va ? body64[ia] : X0;
+    tb = vb ? body64[ib] : X0;
+    eps2 = eps2_;
+    f = reinterpret_cast<float*>(lbase);
+    ff = f + 7 * kGList;
+    lst64 = reinterpret_cast<double4*>(lbase);
     float h, l;
     split_df(ta.x - X0.x, h, l); nhxa = make_float2(-h, -h); nlxa = make_float2(-l, -l);
     split_df(ta.y - X0.y, h, l); nhya = make_float2(-h, -h); nlya = make_float2(-l, -l);
@@ -181,17 +324,34 @@ __device__ __forceinline__ bool group_forces(
     split_df(tb.x - X0.x, h, l); nhxb = make_float2(-h, -h); nlxb = make_float2(-l, -l);
     split_df(tb.y - X0.y, h, l); nhyb = make_float2(-h, -h); nlyb = make_float2(-l, -l);
     split_df(tb.z - X0.z, h, l); nhzb = make_float2(-h, -h); nlzb = make_float2(-l, -l);
+    const float e = (float)eps2;
+    e2 = make_float2(e, e);
+    const float2 z = make_float2(0.f, 0.f);
+    pxa = pya = pza = pxb = pyb = pzb = z;
+    Hx = Hy = Hz = Lx = Ly = Lz = z;
+    ax = ay = az = bx = by = bz = 0.0;
   }
-  const float eps2f = (float)eps2;
-  const float2 e2 = make_float2(eps2f, eps2f);
-  const float2 z2 = make_float2(0.f, 0.f);
-  float2 pxa = z2, pya = z2, pza = z2, pxb = z2, pyb = z2, pzb = z2;  // partials (entry halves)
-  float2 Hx = z2, Hy = z2, Hz = z2, Lx = z2, Ly = z2, Lz = z2;        // (target a, target b)
-  double ax = 0, ay = 0, az = 0, bxs = 0, bys = 0, bzs = 0;          // F64 sums
-  unsigned long long ninter = (unsigned long long)nvalid * (unsigned long long)(nvalid - 1);
-  int listed = 0;  // entries emitted so far
 
-  auto flush = [&]() {
+  // List slot from an absolute position + mass.
+  __device__ __forceinline__ void put(int slot, double4 src) {
+    if (kF32) {
+      float h, l;
+      split_df(src.x - X0.x, h, l);
+      f[slot] = h;
+      f[4 * kGList + slot] = l;
+      split_df(src.y - X0.y, h, l);
+      f[kGList + slot] = h;
+      f[5 * kGList + slot] = l;
+      split_df(src.z - X0.z, h, l);
+      f[2 * kGList + slot] = h;
+      f[6 * kGList + slot] = l;
+      f[3 * kGList + slot] = (float)src.w;
+    } else {
+      lst64[slot] = src;
+    }
+  }
+
+  __device__ __forceinline__ void flush() {
     float2 s, e;
     two_sum2(Hx, make_float2(pxa.x + pxa.y, pxb.x + pxb.y), s, e);
     Hx = s;
@@ -202,14 +362,16 @@ __device__ __forceinline__ bool group_forces(
     two_sum2(Hz, make_float2(pza.x + pza.y, pzb.x + pzb.y), s, e);
     Hz = s;
     Lz = __fadd2_rn(Lz, e);
-    pxa = pya = pza = pxb = pyb = pzb = z2;
-  };
+    const float2 z = make_float2(0.f, 0.f);
+    pxa = pya = pza = pxb = pyb = pzb = z;
+  }
 
   // One F32C entry pair against one target; skip_e / skip_f zero the halves
   // that are the target itself (in-group pass).
-  auto term32 = [&](float2 hx, float2 hy, float2 hz, float2 mm, float2 lx, float2 ly, float2 lz,
-                    float2 nhx, float2 nhy, float2 nhz, float2 nlx, float2 nly, float2 nlz,
-                    bool skip_e, bool skip_f, float2& px, float2& py, float2& pz) {
+  __device__ __forceinline__ void term32(float2 hx, float2 hy, float2 hz, float2 mm, float2 lx,
+                                         float2 ly, float2 lz, float2 nhx, float2 nhy, float2 nhz,
+                                         float2 nlx, float2 nly, float2 nlz, bool skip_e,
+                                         bool skip_f, float2& px, float2& py, float2& pz) {
     const float2 rx = __fadd2_rn(__fadd2_rn(hx, nhx), __fadd2_rn(lx, nlx));
     const float2 ry = __fadd2_rn(__fadd2_rn(hy, nhy), __fadd2_rn(ly, nly));
     const float2 rz = __fadd2_rn(__fadd2_rn(hz, nhz), __fadd2_rn(lz, nlz));
@@ -221,76 +383,74 @@ __device__ __forceinline__ bool group_forces(
     px = __ffma2_rn(rx, w, px);
     py = __ffma2_rn(ry, w, py);
     pz = __ffma2_rn(rz, w, pz);
-  };
+  }
 
-  // F64 entry against one target
-  auto term64 = [&](double4 s, double4 t, double& sx, double& sy, double& sz) {
+  __device__ __forceinline__ void term64(double4 s, double4 t, double& sx, double& sy,
+                                         double& sz) {
     const double rx = s.x - t.x, ry = s.y - t.y, rz = s.z - t.z;
     const double inv = rsqrt(fma(rx, rx, fma(ry, ry, fma(rz, rz, eps2))));
     const double w = s.w * (inv * inv * inv);
     sx = fma(rx, w, sx);
     sy = fma(ry, w, sy);
     sz = fma(rz, w, sz);
-  };
+  }
 
-  // Writes list slot `slot` from an absolute position + mass.
-  auto put = [&](int slot, double4 src) {
-    if (kF32) {
-      float h, l;
-      split_df(src.x - X0.x, h, l);
-      L.hx[slot] = h;
-      L.lx[slot] = l;
-      split_df(src.y - X0.y, h, l);
-      L.hy[slot] = h;
-      L.ly[slot] = l;
-      split_df(src.z - X0.z, h, l);
-      L.hz[slot] = h;
-      L.lz[slot] = l;
-      L.m[slot] = (float)src.w;
-    } else {
-      lst64[slot] = src;
-    }
-  };
-
-  // Evaluates list slots [0, nl) for both targets.
-  auto eval = [&](int nl, bool self) {
+  // Evaluates list slots [0, nl) for both targets (warp-collective).
+  template <bool kSelf>
+  __device__ __forceinline__ void eval(int nl) {
     if (kF32) {
       // pad to a multiple of 4 with massless entries far away
       const int np = (nl + 3) & ~3;
       if (lane < np - nl) {
         const int s = nl + lane;
-        L.hx[s] = L.hy[s] = L.hz[s] = 1e15f;
-        L.m[s] = L.lx[s] = L.ly[s] = L.lz[s] = 0.f;
+        f[s] = f[kGList + s] = f[2 * kGList + s] = 1e15f;
+        f[3 * kGList + s] = f[4 * kGList + s] = f[5 * kGList + s] = f[6 * kGList + s] = 0.f;
       }
       __syncwarp();
       const int nq = np >> 2;
-      const float4* HX = reinterpret_cast<const float4*>(L.hx);
-      const float4* HY = reinterpret_cast<const float4*>(L.hy);
-      const float4* HZ = reinterpret_cast<const float4*>(L.hz);
-      const float4* MM = reinterpret_cast<const float4*>(L.m);
-      const float4* LX = reinterpret_cast<const float4*>(L.lx);
-      const float4* LY = reinterpret_cast<const float4*>(L.ly);
-      const float4* LZ = reinterpret_cast<const float4*>(L.lz);
+      const float4* HX = reinterpret_cast<const float4*>(f);
+      const float4* HY = reinterpret_cast<const float4*>(f + kGList);
+      const float4* HZ = reinterpret_cast<const float4*>(f + 2 * kGList);
+      const float4* MM = reinterpret_cast<const float4*>(f + 3 * kGList);
+      const float4* LX = reinterpret_cast<const float4*>(f + 4 * kGList);
+      const float4* LY = reinterpret_cast<const float4*>(f + 5 * kGList);
+      const float4* LZ = reinterpret_cast<const float4*>(f + 6 * kGList);
       constexpr int kQ = kGFlushPairs / 2;  // 4-entry chunks per flush
-      const int myq = self ? (lane >> 1) : -1;
       for (int q0 = 0; q0 < nq; q0 += kQ) {
         const int q1 = min(q0 + kQ, nq);
 #pragma unroll 2
         for (int q = q0; q < q1; ++q) {
           const float4 hx = HX[q], hy = HY[q], hz = HZ[q], mm = MM[q];
           const float4 lx = LX[q], ly = LY[q], lz = LZ[q];
-          // target a is slot 2*lane, target b slot 2*lane + 1: chunk lane/2,
-          // pair (lane & 1)
-          const bool m0 = q == myq && !(lane & 1);
-          const bool m1 = q == myq && (lane & 1);
+          // in-group pass, the target's own slot: two per lane: target a is
+          // slot 2*lane, target b 2*lane + 1 (chunk lane/2, pair lane & 1);
+          // one per lane: slot lane (chunk lane/4, pair (lane/2) & 1, half
+          // lane & 1)
+          bool a0e = false, a0f = false, a1e = false, a1f = false, b0 = false, b1 = false;
+          if (kSelf) {
+            if (two) {
+              const bool in = q == (lane >> 1);
+              a0e = b0 = in && !(lane & 1);
+              a1e = b1 = in && (lane & 1);
+            } else {
+              const bool in = q == (lane >> 2);
+              const bool p1 = (lane >> 1) & 1, h1 = lane & 1;
+              a0e = in && !p1 && !h1;
+              a0f = in && !p1 && h1;
+              a1e = in && p1 && !h1;
+              a1f = in && p1 && h1;
+            }
+          }
           term32(lo2(hx), lo2(hy), lo2(hz), lo2(mm), lo2(lx), lo2(ly), lo2(lz), nhxa, nhya, nhza,
-                 nlxa, nlya, nlza, m0, false, pxa, pya, pza);
-          term32(lo2(hx), lo2(hy), lo2(hz), lo2(mm), lo2(lx), lo2(ly), lo2(lz), nhxb, nhyb, nhzb,
-                 nlxb, nlyb, nlzb, false, m0, pxb, pyb, pzb);
+                 nlxa, nlya, nlza, a0e, a0f, pxa, pya, pza);
           term32(hi2(hx), hi2(hy), hi2(hz), hi2(mm), hi2(lx), hi2(ly), hi2(lz), nhxa, nhya, nhza,
-                 nlxa, nlya, nlza, m1, false, pxa, pya, pza);
-          term32(hi2(hx), hi2(hy), hi2(hz), hi2(mm), hi2(lx), hi2(ly), hi2(lz), nhxb, nhyb, nhzb,
-                 nlxb, nlyb, nlzb, false, m1, pxb, pyb, pzb);
+                 nlxa, nlya, nlza, a1e, a1f, pxa, pya, pza);
+          if (two) {
+            term32(lo2(hx), lo2(hy), lo2(hz), lo2(mm), lo2(lx), lo2(ly), lo2(lz), nhxb, nhyb,
+                   nhzb, nlxb, nlyb, nlzb, false, b0, pxb, pyb, pzb);
+            term32(hi2(hx), hi2(hy), hi2(hz), hi2(mm), hi2(lx), hi2(ly), hi2(lz), nhxb, nhyb,
+                   nhzb, nlxb, nlyb, nlzb, false, b1, pxb, pyb, pzb);
+          }
         }
         flush();
       }
@@ -299,101 +459,369 @@ __device__ __forceinline__ bool group_forces(
 #pragma unroll 2
       for (int e = 0; e < nl; ++e) {
         const double4 s = lst64[e];
-        if (!(self && e == 2 * lane)) term64(s, ta, ax, ay, az);
-        if (!(self && e == 2 * lane + 1)) term64(s, tb, bxs, bys, bzs);
+        if (!(kSelf && e == (two ? 2 * lane : lane))) term64(s, ta, ax, ay, az);
+        if (two && !(kSelf && e == 2 * lane + 1)) term64(s, tb, bx, by, bz);
       }
     }
     __syncwarp();
-  };
+  }
 
-  // ---- pairs inside the group (exact, i != j) ----
-  if (va) put(2 * lane, ta);
-  if (vb) put(2 * lane + 1, tb);
-  eval(nvalid, true);
+  // One far F32C entry pair against one target: plain f32 offsets from X0.
+  __device__ __forceinline__ void term32f(float2 hx, float2 hy, float2 hz, float2 mm,
+                                          float2 nhx, float2 nhy, float2 nhz, float2& px,
+                                          float2& py, float2& pz) {
+    const float2 rx = __fadd2_rn(hx, nhx);
+    const float2 ry = __fadd2_rn(hy, nhy);
+    const float2 rz = __fadd2_rn(hz, nhz);
+    const float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, e2)));
+    const float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 w = __fmul2_rn(mm, __fmul2_rn(__fmul2_rn(inv, inv), inv));
+    px = __ffma2_rn(rx, w, px);
+    py = __ffma2_rn(ry, w, py);
+    pz = __ffma2_rn(rz, w, pz);
+  }
 
-  // ---- tree walk ----
-  int ssize = 1, lsize = 0;
-  long long pops = 0;
-  if (lane == 0) stk[0] = 0;
-  __syncwarp();
-  while (ssize > 0) {
-    if (listed > limit) return false;
-    const int k = ssize <= kGThrottle - 7 ? min(min(32, ssize), (kGThrottle - ssize) / 7) : 1;
-    const int nd = lane < k ? stk[ssize - 1 - lane] : -1;
-    ssize -= k;
-    pops += k;
+  // Evaluates far-list slots [0, nl) for both targets (warp-collective).
+  __device__ __forceinline__ void eval_far(int nl) {
+    const int np = (nl + 3) & ~3;
+    if (lane < np - nl) {
+      const int s = nl + lane;
+      ff[s] = ff[kGList + s] = ff[2 * kGList + s] = 1e15f;
+      ff[3 * kGList + s] = 0.f;
+    }
     __syncwarp();
-    int npush = 0, cfirst = 0, nent = 0, kind = 0, a = 0, olo = 0, ohi = 0;
-    bool malformed = pops > nnodes;
-    if (nd >= 0) {
-      const GNode* g = gn + nd;
-      const int4 l = __ldg(&g->l);
-      const int type = l.y & 3, cnt = l.y >> 2;
-      const bool inside = l.z >= base && l.w <= gend;  // only group bodies
-      if (type == kGSkip || inside) {
-      } else if (type == kGSingle) {
-        if (l.x < base || l.x >= gend) {
-          nent = 1;
-          kind = 1;
-          a = nd;
-        }
-      } else {
-        const bool overlap = l.z < gend && l.w > base;
-        bool acc = false;
-        if (!overlap) {
-          const float4 h = __ldg(&g->hi), lo = __ldg(&g->lo);
-          const float rx = (h.x - x0hx) + (lo.x - x0lx);
-          const float ry = (h.y - x0hy) + (lo.y - x0ly);
-          const float rz = (h.z - x0hz) + (lo.z - x0lz);
-          const float dx = fmaxf(fabsf(rx - cx) - bx, 0.f);
-          const float dy = fmaxf(fabsf(ry - cy) - by, 0.f);
-          const float dz = fmaxf(fabsf(rz - cz) - bz, 0.f);
-          const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          acc = lo.w < theta2f * d2 * (1.0f - 1e-5f);
-        }
-        if (acc) {
-          nent = 1;
-          kind = 1;
-          a = nd;
-        } else if (type == kGInternal) {
-          if (l.x <= nd || cnt < 1 || cnt > 8 || l.x + cnt > nnodes) {
-            malformed = true;
-          } else {
-            npush = cnt;
-            cfirst = l.x;
-          }
-        } else {  // bucket leaf opened: its bodies outside the group
-          a = l.z;
-          olo = max(l.z, base);
-          ohi = min(l.w, gend);
-          nent = (l.w - l.z) - max(ohi - olo, 0);
-          kind = 2;
+    const int nq = np >> 2;
+    const float4* HX = reinterpret_cast<const float4*>(ff);
+    const float4* HY = reinterpret_cast<const float4*>(ff + kGList);
+    const float4* HZ = reinterpret_cast<const float4*>(ff + 2 * kGList);
+    const float4* MM = reinterpret_cast<const float4*>(ff + 3 * kGList);
+    constexpr int kQ = kGFlushPairs / 2;
+    for (int q0 = 0; q0 < nq; q0 += kQ) {
+      const int q1 = min(q0 + kQ, nq);
+#pragma unroll 2
+      for (int q = q0; q < q1; ++q) {
+        const float4 hx = HX[q], hy = HY[q], hz = HZ[q], mm = MM[q];
+        term32f(lo2(hx), lo2(hy), lo2(hz), lo2(mm), nhxa, nhya, nhza, pxa, pya, pza);
+        term32f(hi2(hx), hi2(hy), hi2(hz), hi2(mm), nhxa, nhya, nhza, pxa, pya, pza);
+        if (two) {
+          term32f(lo2(hx), lo2(hy), lo2(hz), lo2(mm), nhxb, nhyb, nhzb, pxb, pyb, pzb);
+          term32f(hi2(hx), hi2(hy), hi2(hz), hi2(mm), nhxb, nhyb, nhzb, pxb, pyb, pzb);
         }
       }
+      flush();
     }
-    const int pin = warp_incl_scan(npush, lane);
-    const int ptot = __shfl_sync(kFull, pin, 31);
-    if (__any_sync(kFull, malformed) || ssize + ptot > kGStack) {
+    __syncwarp();
+  }
+
+  // Gathers list entries [0, nb) of `codes` (warp-collective) and evaluates
+  // them.  F32C: an entry whose distance from the group's box is at least
+  // GWALK_FAR box half-diagonals b goes to the far list, whose plain f32
+  // offsets from X0 need no low parts: targets lie within 2b of X0, so the
+  // separation's error is below 2^-24 (2|r| + 4b) <= 6 * 2^-24 |r|, the
+  // size of the f32 pair term's own rounding; the rest go to the near list
+  // (double-float).
+  __device__ __forceinline__ void gather_eval(const uint32_t* __restrict__ codes, int nb,
+                                              const GNode* __restrict__ gn,
+                                              const double4* __restrict__ body64, const Box& B,
+                                              float far2) {
+    if (!kF32) {
+#pragma unroll 4
+      for (int e = lane; e < nb; e += 32) {
+        const uint32_t code = codes[e];
+        const int id = (int)(code >> 1);
+        put(e, (code & 1u) ? ldg_d4(&body64[id]) : ldg_d4(&gn[id].c64));
+      }
+      eval<false>(nb);
+      return;
+    }
+    int nnear = 0, nfar = 0;
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll 2
+    for (int e0 = 0; e0 < nb; e0 += 32) {
+      const int e = e0 + lane;
+      const bool valid = e < nb;
+      double4 src = make_double4(0.0, 0.0, 0.0, 0.0);
+      if (valid) {
+        const uint32_t code = codes[e];
+        const int id = (int)(code >> 1);
+        src = (code & 1u) ? ldg_d4(&body64[id]) : ldg_d4(&gn[id].c64);
+      }
+      float hx, lx, hy, ly, hz, lz;
+      split_df(src.x - X0.x, hx, lx);
+      split_df(src.y - X0.y, hy, ly);
+      split_df(src.z - X0.z, hz, lz);
+      const float dx = fmaxf(fabsf(hx - B.cx) - B.bx, 0.f);
+      const float dy = fmaxf(fabsf(hy - B.cy) - B.by, 0.f);
+      const float dz = fmaxf(fabsf(hz - B.cz) - B.bz, 0.f);
+      const bool far = valid && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) >= far2;
+      const unsigned fm = __ballot_sync(kFull, far);
+      const unsigned nm = __ballot_sync(kFull, valid && !far);
+      const float m = (float)src.w;
+      if (far) {
+        const int q = nfar + __popc(fm & lt);
+        ff[q] = hx;
+        ff[kGList + q] = hy;
+        ff[2 * kGList + q] = hz;
+        ff[3 * kGList + q] = m;
+      } else if (valid) {
+        const int q = nnear + __popc(nm & lt);
+        f[q] = hx;
+        f[kGList + q] = hy;
+        f[2 * kGList + q] = hz;
+        f[3 * kGList + q] = m;
+        f[4 * kGList + q] = lx;
+        f[5 * kGList + q] = ly;
+        f[6 * kGList + q] = lz;
+      }
+      nfar += __popc(fm);
+      nnear += __popc(nm);
+    }
+    if (nnear) eval<false>(nnear);
+    if (nfar) eval_far(nfar);
+  }
+
+  // Pairs inside the group, exact, i != j.
+  __device__ __forceinline__ void self_pass() {
+    if (va) put(two ? 2 * lane : lane, ta);
+    if (vb) put(2 * lane + 1, tb);
+    eval<true>(nvalid);
+  }
+
+  __device__ __forceinline__ void finish(const double4* __restrict__ body64,
+                                         const uint32_t* __restrict__ perm, double G,
+                                         int want_force, double* __restrict__ ox,
+                                         double* __restrict__ oy, double* __restrict__ oz,
+                                         int32_t* status) {
+    auto out = [&](int pp, double fx, double fy, double fz) {
+      const double sc = want_force ? G * body64[pp].w : G;
+      fx *= sc;
+      fy *= sc;
+      fz *= sc;
+      const uint32_t i = perm[pp];
+      ox[i] = fx;
+      oy[i] = fy;
+      oz[i] = fz;
+      if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz)) atomicOr(status, kStatNonfinite);
+    };
+    if (kF32) {
+      if (va) out(ia, (double)Hx.x + (double)Lx.x, (double)Hy.x + (double)Ly.x,
+                  (double)Hz.x + (double)Lz.x);
+      if (vb) out(ib, (double)Hx.y + (double)Lx.y, (double)Hy.y + (double)Ly.y,
+                  (double)Hz.y + (double)Lz.y);
+    } else {
+      if (va) out(ia, ax, ay, az);
+      if (vb) out(ib, bx, by, bz);
+    }
+  }
+};
+
+// Takes the next work index for the warp.
+__device__ __forceinline__ int next_item(int lane, int32_t* ctr) {
+  int gi = 0;
+  if (lane == 0) gi = atomicAdd(ctr, 1);
+  return __shfl_sync(kFull, gi, 0);
+}
+
+__device__ __forceinline__ bool bad_range(int2 gr, int n) {
+  return gr.x < 0 || gr.y > n || gr.y - gr.x < 1 || gr.y - gr.x > kGroupMax;
+}
+
+// Re-queues [gr.x, gr.y) as subgroups of kGSplit bodies (lane 0).  The
+// subgroups are disjoint and non-empty: at most n of them in all.
+__device__ __forceinline__ bool requeue(int2 gr, int n, int2* retry, int32_t* nretry) {
+  const int nsub = (gr.y - gr.x + kGSplit - 1) / kGSplit;
+  const int at = atomicAdd(nretry, nsub);
+  bool ok = true;
+  for (int k = 0; k < nsub; ++k) {
+    if (at + k < n) {
+      retry[at + k] = make_int2(gr.x + k * kGSplit, min(gr.x + (k + 1) * kGSplit, gr.y));
+    } else {
+      ok = false;
+    }
+  }
+  return ok;
+}
+
+// ---------------------------------------------------------------------------
+// 1. lists.  Entry codes: cell record nd -> nd << 1; body q -> q << 1 | 1.
+// Items: n int4 {first body, end body, 0, list length}, then n int64 pool
+// offsets.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kLBlock)
+glist_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __restrict__ groups,
+             const int32_t* __restrict__ ngroups_p, int32_t* __restrict__ ctr,
+             const double4* __restrict__ body64, float theta2f, uint32_t* __restrict__ pool,
+             int64_t pool_per_warp, int4* __restrict__ items, int32_t* __restrict__ nitems,
+             int2* __restrict__ retry, int32_t* __restrict__ nretry, int32_t* status) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int* stk = reinterpret_cast<int*>(gsm) + wid * kGStack;
+  const int64_t region0 = (blockIdx.x * (int64_t)kLWarps + wid) * pool_per_warp;
+  uint32_t* region = pool + region0;
+  const int cap = (int)min64(pool_per_warp, (int64_t)INT_MAX);
+  int64_t* offs = reinterpret_cast<int64_t*>(items + n);
+  const int ngroups = min(*ngroups_p, n);
+  int roff = 0;  // used part of the region
+  bool bad = false;
+  for (;;) {
+    const int gi = next_item(lane, ctr);
+    if (gi >= ngroups) break;
+    const int2 gr = groups[gi];
+    if (bad_range(gr, n)) {
       bad = true;
       break;
     }
-    for (int c = 0; c < npush; ++c) stk[ssize + pin - npush + c] = cfirst + c;
-    ssize += ptot;
-    __syncwarp();  // pushes visible to the next round's pops
-    const int ein = warp_incl_scan(nent, lane);
-    const int etot = __shfl_sync(kFull, ein, 31);
-    listed += etot;
-    if (etot > 0) {
-      r_end[lane] = ein;
-      r_kind[lane] = kind;
-      r_a[lane] = a;
-      r_olo[lane] = olo;
-      r_ohi[lane] = ohi;
+    const int base = gr.x, gend = gr.y;
+    const double4 X0 = body64[base];
+    const int ia = base + 2 * lane, ib = ia + 1;
+    const double4 ta = ia < gend ? body64[ia] : X0;
+    const double4 tb = ib < gend ? body64[ib] : X0;
+    const Box B = group_box(X0, ta, tb);
+    int used = 0;
+    auto sink = [&](int etot, int eoff, const NodeOut& o) -> bool {
+      if (roff + used + etot > cap) return false;  // region full: re-queue
+      uint32_t* dst = region + roff + used + eoff;
+      if (o.kind == 1) {
+        dst[0] = (uint32_t)o.a << 1;
+      } else {
+        for (int j = 0; j < o.nent; ++j)
+          dst[j] = ((uint32_t)bucket_body(o.a, o.olo, o.ohi, j) << 1) | 1u;
+      }
+      used += etot;
+      return true;
+    };
+    const int r = traverse<false>(lane, base, gend, nnodes, kGListLimit, stk, B, theta2f, gn,
+                                  sink);
+    if (r < 0) {
+      bad = true;
+      break;
+    }
+    if (lane == 0) {
+      if (r == 1) {
+        const int it = atomicAdd(nitems, 1);
+        if (it < n) {
+          items[it] = make_int4(base, gend, 0, used);
+          offs[it] = region0 + roff;
+        } else {
+          bad = true;
+        }
+      } else if (!requeue(gr, n, retry, nretry)) {
+        bad = true;
+      }
+    }
+    if (r == 1) roff += used;
+    __syncwarp();
+  }
+  if (bad && lane == 0) atomicOr(status, kStatOverflow);
+}
+
+// ---------------------------------------------------------------------------
+// 2. evaluation of the lists
+// ---------------------------------------------------------------------------
+template <bool kF32>
+__global__ void __launch_bounds__(kGBlock, 4)
+geval_kernel(int n, const GNode* __restrict__ gn, const int4* __restrict__ items,
+             const int32_t* __restrict__ nitems_p, int32_t* __restrict__ ctr,
+             const uint32_t* __restrict__ pool, const double4* __restrict__ body64,
+             const uint32_t* __restrict__ perm, double G, double eps2, int want_force,
+             double* __restrict__ ox, double* __restrict__ oy, double* __restrict__ oz,
+             unsigned long long* counter, int32_t* status) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned char* lbase = gsm + wid * kESmemWarp;
+  const int nitems = min(*nitems_p, n);
+  const int64_t* offs = reinterpret_cast<const int64_t*>(items + n);
+  unsigned long long ninter = 0;
+  for (;;) {
+    const int it = next_item(lane, ctr);
+    if (it >= nitems) break;
+    const int4 item = items[it];
+    const uint32_t* codes = pool + offs[it];
+    const int len = item.w;
+    Evaluator<kF32> E;
+    E.init(lane, item.x, item.y, body64, lbase, eps2);
+    const Box B = group_box(E.X0, E.ta, E.tb);
+    const float far2 = (float)(GWALK_FAR * GWALK_FAR) * fmaf(B.bx, B.bx, fmaf(B.by, B.by, B.bz * B.bz));
+    E.self_pass();
+    ninter += (unsigned long long)E.nvalid * (unsigned long long)(E.nvalid - 1 + len);
+    for (int b0 = 0; b0 < len; b0 += kGList)
+      E.gather_eval(codes + b0, min(kGList, len - b0), gn, body64, B, far2);
+    E.finish(body64, perm, G, want_force, ox, oy, oz, status);
+  }
+  if (lane == 0 && ninter) atomicAdd(counter, ninter);  // the same on every lane
+}
+
+// ---------------------------------------------------------------------------
+// 3. walk + evaluation in one pass (re-queued subgroups)
+// ---------------------------------------------------------------------------
+template <bool kF32>
+__global__ void __launch_bounds__(kGBlock, 4)
+gwalk_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __restrict__ groups,
+             const int32_t* __restrict__ ngroups_p, int32_t* __restrict__ ctr,
+             const double4* __restrict__ body64, const uint32_t* __restrict__ perm, double G,
+             double eps2, float theta2f, int want_force, double* __restrict__ ox,
+             double* __restrict__ oy, double* __restrict__ oz, unsigned long long* counter,
+             int32_t* status) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned char* ws = gsm + wid * kGSmemWarp;
+  int* stk = reinterpret_cast<int*>(ws);
+  int* rec = reinterpret_cast<int*>(ws + kGRecOff);
+  int* r_end = rec;
+  int* r_kind = rec + 32;
+  int* r_a = rec + 64;
+  int* r_olo = rec + 96;
+  int* r_ohi = rec + 128;
+  double4* r_src = reinterpret_cast<double4*>(rec + 160);
+  const int ngroups = min(*ngroups_p, n);
+  unsigned long long ninter = 0;
+  bool bad = false;
+  for (;;) {
+    const int gi = next_item(lane, ctr);
+    if (gi >= ngroups) break;
+    const int2 gr = groups[gi];
+    if (bad_range(gr, n)) {
+      bad = true;
+      break;
+    }
+    Evaluator<kF32> E;
+    E.init(lane, gr.x, gr.y, body64, ws + kGListOff, eps2);
+    const Box B = group_box(E.X0, E.ta, E.tb);
+    E.self_pass();
+    const unsigned long long nv = (unsigned long long)E.nvalid;
+    unsigned long long ni = nv * (nv - 1);
+    int lsize = 0;
+    auto sink = [&](int etot, int eoff, const NodeOut& o) -> bool {
+      if (lsize + etot > kGList && lsize > 0) {
+        E.template eval<false>(lsize);
+        ni += (unsigned long long)lsize * nv;
+        lsize = 0;
+      }
+      if (etot <= kGList) {
+        // every lane writes its own entries at its scan offset
+        const int s0 = lsize + eoff;
+        if (o.kind == 1) {
+          E.put(s0, o.c64);
+        } else {
+          for (int j = 0; j < o.nent; ++j)
+            E.put(s0 + j, ldg_d4(&body64[bucket_body(o.a, o.olo, o.ohi, j)]));
+        }
+        lsize += etot;
+        return true;
+      }
+      // more entries than the list holds (a leaf of many bodies at the guard
+      // depth): windows of kGList entries spread over the lanes
+      r_end[lane] = eoff + o.nent;
+      r_kind[lane] = o.kind;
+      r_src[lane] = o.c64;
+      r_a[lane] = o.a;
+      r_olo[lane] = o.olo;
+      r_ohi[lane] = o.ohi;
       __syncwarp();
       for (int done = 0; done < etot;) {
         if (lsize == kGList) {
-          eval(lsize, false);
-          ninter += (unsigned long long)lsize * (unsigned long long)nvalid;
+          E.template eval<false>(lsize);
+          ni += (unsigned long long)lsize * nv;
           lsize = 0;
         }
         const int take = min(etot - done, kGList - lsize);
@@ -406,104 +834,28 @@ __device__ __forceinline__ bool group_forces(
             else lo = mid + 1;
           }
           const int j = e - (lo ? r_end[lo - 1] : 0);
-          double4 src;
-          if (r_kind[lo] == 1) {
-            src = ldg_d4(&gn[r_a[lo]].c64);
-          } else {
-            int q = r_a[lo] + j;
-            const int ol = r_olo[lo], oh = r_ohi[lo];
-            if (ol < oh && q >= ol) q += oh - ol;
-            src = ldg_d4(&body64[q]);
-          }
-          put(lsize + (e - done), src);
+          const double4 src = r_kind[lo] == 1
+                                  ? r_src[lo]
+                                  : ldg_d4(&body64[bucket_body(r_a[lo], r_olo[lo], r_ohi[lo], j)]);
+          E.put(lsize + (e - done), src);
         }
         lsize += take;
         done += take;
       }
       __syncwarp();
-    }
-  }
-  if (bad) return true;
-  if (lsize > 0) {
-    eval(lsize, false);
-    ninter += (unsigned long long)lsize * (unsigned long long)nvalid;
-  }
-  ninter_out += ninter;
-
-  auto out = [&](int pp, double fx, double fy, double fz) {
-    const double sc = want_force ? G * body64[pp].w : G;
-    fx *= sc;
-    fy *= sc;
-    fz *= sc;
-    const uint32_t i = perm[pp];
-    ox[i] = fx;
-    oy[i] = fy;
-    oz[i] = fz;
-    if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz)) atomicOr(status, kStatNonfinite);
-  };
-  if (kF32) {
-    if (va) out(ia, (double)Hx.x + (double)Lx.x, (double)Hy.x + (double)Ly.x,
-                (double)Hz.x + (double)Lz.x);
-    if (vb) out(ib, (double)Hx.y + (double)Lx.y, (double)Hy.y + (double)Ly.y,
-                (double)Hz.y + (double)Lz.y);
-  } else {
-    if (va) out(ia, ax, ay, az);
-    if (vb) out(ib, bxs, bys, bzs);
-  }
-  return true;
-}
-
-// Persistent warps: each takes the next group from the counter until none
-// is left.  First pass (retry != nullptr): a group whose list passes
-// kGListLimit entries is abandoned and re-queued as subgroups of kGSplit
-// consecutive bodies (a group whose box reaches a much denser region; its
-// small subgroups have far shorter lists).  Second pass: the re-queued
-// subgroups, without a limit.
-template <bool kF32>
-__global__ void __launch_bounds__(kGBlock)
-gwalk_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __restrict__ groups,
-             const int32_t* __restrict__ ngroups_p, int32_t* __restrict__ ctr,
-             int2* __restrict__ retry, int32_t* __restrict__ nretry,
-             const double4* __restrict__ body64, const uint32_t* __restrict__ perm, double G,
-             double eps2, float theta2f, int want_force, double* __restrict__ ox,
-             double* __restrict__ oy, double* __restrict__ oz, unsigned long long* counter,
-             int32_t* status) {
-  extern __shared__ __align__(16) unsigned char gsm[];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  unsigned char* ws = gsm + wid * kGSmemWarp;
-  int* stk = reinterpret_cast<int*>(ws);
-  int* rec = reinterpret_cast<int*>(ws + kGRecOff);
-  const int ngroups = min(*ngroups_p, n);
-  const int limit = retry ? kGListLimit : INT_MAX;
-  unsigned long long ninter = 0;
-  bool bad = false;
-  for (;;) {
-    int gi = 0;
-    if (lane == 0) gi = atomicAdd(ctr, 1);
-    gi = __shfl_sync(kFull, gi, 0);
-    if (gi >= ngroups) break;
-    const int2 gr = groups[gi];
-    if (gr.x < 0 || gr.y > n || gr.y - gr.x < 1 || gr.y - gr.x > kGroupMax) {
+      return true;
+    };
+    const int r = traverse<true>(lane, gr.x, gr.y, nnodes, INT_MAX, stk, B, theta2f, gn, sink);
+    if (r != 1) {
       bad = true;
       break;
     }
-    const bool done =
-        group_forces<kF32>(lane, gr.x, gr.y, nnodes, limit, stk, ws + kGListOff, rec, gn, body64,
-                           perm, G, eps2, theta2f, want_force, ox, oy, oz, ninter, bad, status);
-    if (bad) break;
-    if (!done && lane == 0) {
-      // subgroups are disjoint and non-empty: at most n of them in all
-      const int nsub = (gr.y - gr.x + kGSplit - 1) / kGSplit;
-      const int at = atomicAdd(nretry, nsub);
-      for (int k = 0; k < nsub; ++k) {
-        if (at + k < n) {
-          retry[at + k] = make_int2(gr.x + k * kGSplit, min(gr.x + (k + 1) * kGSplit, gr.y));
-        } else {
-          bad = true;
-        }
-      }
+    if (lsize > 0) {
+      E.template eval<false>(lsize);
+      ni += (unsigned long long)lsize * nv;
     }
-    __syncwarp();
+    ninter += ni;
+    E.finish(body64, perm, G, want_force, ox, oy, oz, status);
   }
   if (lane == 0) {
     if (bad) atomicOr(status, kStatOverflow);
@@ -511,34 +863,56 @@ gwalk_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __rest
   }
 }
 
+// Resident blocks per SM of a kernel with its dynamic shared memory (cached
+// per kernel: its resources are fixed).
+template <class K>
+int occupancy(phys_ctx* c, K kernel, int block, int smem, int* cache) {
+  if (!*cache) {
+    PHYS_CUDA(c, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int b = 0;
+    PHYS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, block, smem));
+    *cache = b > 0 ? b : 1;
+  }
+  return PHYS_OK;
+}
+
 template <bool kF32>
 int launch(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force, double* ox,
            double* oy, double* oz) {
-  static int blocks_per_sm = 0;  // per process; the kernel and its resources are fixed
-  if (!blocks_per_sm) {
-    PHYS_CUDA(c, cudaFuncSetAttribute(gwalk_kernel<kF32>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
-    int b = 0;
-    PHYS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, gwalk_kernel<kF32>, kGBlock,
-                                                               kGSmem));
-    blocks_per_sm = b > 0 ? b : 1;
-  }
+  static int occ_list = 0, occ_eval = 0, occ_fused = 0;
+  PHYS_TRY(occupancy(c, glist_kernel, kLBlock, kLSmem, &occ_list));
+  PHYS_TRY(occupancy(c, geval_kernel<kF32>, kGBlock, kESmem, &occ_eval));
+  PHYS_TRY(occupancy(c, gwalk_kernel<kF32>, kGBlock, kGSmem, &occ_fused));
   int sms = 0;
   PHYS_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-  const int64_t max_blocks = ceil_div(t.n, (int64_t)kGWarps);
-  const int grid = (int)min64((int64_t)sms * blocks_per_sm, max_blocks);
-  // group_ctr: [0] first-pass counter, [1] second-pass counter, [2] re-queued count
-  PHYS_CUDA(c, cudaMemsetAsync(t.group_ctr, 0, 3 * sizeof(int32_t), c->stream));
+  const int64_t n = t.n;
+  const int grid_list = (int)min64((int64_t)sms * occ_list, ceil_div(n, (int64_t)kLWarps));
+  const int grid_eval = (int)min64((int64_t)sms * occ_eval, ceil_div(n, (int64_t)kGWarps));
+  const int grid_fused = (int)min64((int64_t)sms * occ_fused, ceil_div(n, (int64_t)kGWarps));
+  // list pool: one region per list warp, each at least one full list
+  const int64_t warps = (int64_t)grid_list * kLWarps;
+  const int64_t pool_per_warp = std::max((int64_t)kGListLimit + 64,
+                                         ceil_div(n * (int64_t)GWALK_POOL_PER_BODY, warps));
+  uint32_t* pool = nullptr;
+  int4* items = nullptr;  // n int4 items, then n int64 pool offsets
+  PHYS_TRY(ws_alloc(c, WS_GROUP_POOL, warps * pool_per_warp, &pool));
+  PHYS_TRY(ws_alloc(c, WS_GROUP_ITEMS, 2 * n, &items));
+  // group_ctr: [0] list counter, [1] re-queued count, [2] items, [3]
+  // evaluation counter, [4] second-walk counter
+  int32_t* ctr = t.group_ctr;
+  PHYS_CUDA(c, cudaMemsetAsync(ctr, 0, 5 * sizeof(int32_t), c->stream));
   const double eps2 = p->eps * p->eps;
   const float theta2f = (float)(p->theta * p->theta);
-  int2* retry = const_cast<int2*>(t.groups) + t.n;
-  PHYS_LAUNCH(c, gwalk_kernel<kF32>, grid, kGBlock, kGSmem, (int)t.n, (int)t.nnodes, t.gnode,
-              t.groups, t.ngroups, t.group_ctr, retry, t.group_ctr + 2, t.body64, t.perm, p->G,
-              eps2, theta2f, (int)want_force, ox, oy, oz, c->d_counter, c->d_status);
-  PHYS_LAUNCH(c, gwalk_kernel<kF32>, grid, kGBlock, kGSmem, (int)t.n, (int)t.nnodes, t.gnode,
-              retry, t.group_ctr + 2, t.group_ctr + 1, (int2*)nullptr, (int32_t*)nullptr,
-              t.body64, t.perm, p->G, eps2, theta2f, (int)want_force, ox, oy, oz, c->d_counter,
-              c->d_status);
+  int2* retry = const_cast<int2*>(t.groups) + n;
+  PHYS_LAUNCH(c, glist_kernel, grid_list, kLBlock, kLSmem, (int)n, (int)t.nnodes, t.gnode,
+              t.groups, t.ngroups, ctr, t.body64, theta2f, pool, pool_per_warp, items, ctr + 2,
+              retry, ctr + 1, c->d_status);
+  PHYS_LAUNCH(c, geval_kernel<kF32>, grid_eval, kGBlock, kESmem, (int)n, t.gnode, items, ctr + 2,
+              ctr + 3, pool, t.body64, t.perm, p->G, eps2, (int)want_force, ox, oy, oz,
+              c->d_counter, c->d_status);
+  PHYS_LAUNCH(c, gwalk_kernel<kF32>, grid_fused, kGBlock, kGSmem, (int)n, (int)t.nnodes, t.gnode,
+              retry, ctr + 1, ctr + 4, t.body64, t.perm, p->G, eps2, theta2f, (int)want_force, ox,
+              oy, oz, c->d_counter, c->d_status);
   return PHYS_OK;
 }
 
@@ -547,7 +921,7 @@ int launch(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force, 
 int bh_group_walk(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force,
                   double* ox, double* oy, double* oz) {
   if (!t.gnode || !t.groups) return fail(c, PHYS_ERR_STATE, "group walk without group records");
-  if (t.n > INT32_MAX - kGroupMax || t.nnodes > INT32_MAX)
+  if (t.n > INT32_MAX / 2 - kGroupMax || t.nnodes > INT32_MAX / 2)
     return fail(c, PHYS_ERR_ARG, "group walk: %lld bodies is too many", (long long)t.n);
   return p->precision == PHYS_F32C ? launch<true>(c, p, t, want_force, ox, oy, oz)
                                    : launch<false>(c, p, t, want_force, ox, oy, oz);

@@ -884,7 +884,7 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
     PHYS_TRY(ws_alloc(c, WS_NCOUNT, nnodes + 1, &gcnt));
     PHYS_TRY(ws_alloc(c, WS_GROUP_OFF, nnodes + 1, &goff));
     PHYS_TRY(ws_alloc(c, WS_GROUPS, 2 * n, &groups));  // groups, then re-queued subgroups
-    PHYS_TRY(ws_alloc(c, WS_GROUP_CTR, 3, &gctr));
+    PHYS_TRY(ws_alloc(c, WS_GROUP_CTR, 8, &gctr));
     PHYS_LAUNCH(c, group_kernel<false>, grid_for(nnodes + 1), kBlock, 0, nnodes, bfs2pre, link,
                 nchild, gcnt, goff, groups, n);
     PHYS_TRY(scan_exclusive_i32(c, gcnt, goff, nnodes + 1));
