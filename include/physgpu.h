@@ -95,6 +95,10 @@ typedef struct phys_timings {
   int64_t nodes;        /* octree nodes of the last BH evaluation             */
   int32_t max_depth;    /* guard depth D* of the last BH tree                 */
   int32_t reserved;
+  double walk_eval_ms;  /* group walk: the list-evaluation kernel alone (part
+                           of walk_ms); 0 for the other walks              */
+  uint64_t walk_eval_interactions; /* group walk: interactions evaluated by
+                           that kernel (the rest: re-queued subgroups)      */
 } phys_timings;
 
 /* ---- context ------------------------------------------------------------ */

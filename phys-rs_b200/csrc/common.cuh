@@ -60,6 +60,7 @@ struct phys_ctx {
   bool accel_valid = false;
   phys_params accel_params{};
   bool last_eval_bh = false;   // the interaction count lives in d_counter
+  bool last_eval_group = false;  // ev[10], ev[11] bracket the group walk's list evaluation
 
   // ---- batched ensemble (independent small systems) ----
   int64_t ens_nsys = 0, ens_nbody = 0;

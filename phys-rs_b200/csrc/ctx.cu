@@ -79,14 +79,15 @@ int ensure_pinned(phys_ctx* c, size_t bytes) {
 int read_status(phys_ctx* c, int32_t* out) {
   PHYS_CUDA(c, cudaMemcpyAsync(c->h_small, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost,
                                c->stream));
-  PHYS_CUDA(c, cudaMemcpyAsync(c->h_small + 2, c->d_counter, sizeof(unsigned long long),
+  PHYS_CUDA(c, cudaMemcpyAsync(c->h_small + 2, c->d_counter, 2 * sizeof(unsigned long long),
                                cudaMemcpyDeviceToHost, c->stream));
   PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
   *out = c->h_small[0];
   if (c->last_eval_bh) {
-    unsigned long long v;
-    memcpy(&v, c->h_small + 2, sizeof v);
-    c->tm.interactions = v;
+    unsigned long long v[2];
+    memcpy(v, c->h_small + 2, sizeof v);
+    c->tm.interactions = v[0];
+    c->tm.walk_eval_interactions = c->last_eval_group ? v[1] : 0;
   }
   return PHYS_OK;
 }
@@ -168,6 +169,7 @@ int eval(phys_ctx* c, const phys_params* p, bool want_force) {
     return PHYS_OK;
   }
   c->last_eval_bh = p->method == PHYS_BARNES_HUT;
+  c->last_eval_group = c->last_eval_bh && (p->flags & PHYS_FLAG_GROUP_WALK);
   if (p->method == PHYS_DIRECT) return direct_eval(c, p, want_force, ox, oy, oz);
   return bh_eval(c, p, want_force, ox, oy, oz);
 }
@@ -184,6 +186,7 @@ int finish_status(phys_ctx* c) {
     c->tm.tree_ms = ev_ms(c->ev[5], c->ev[6]);
   }
   c->tm.walk_ms = ev_ms(c->ev[6], c->ev[7]);
+  c->tm.walk_eval_ms = c->last_eval_group ? ev_ms(c->ev[10], c->ev[11]) : 0.0;
   if (st & kStatTimeout) return fail(c, PHYS_ERR_TIMEOUT, "a bounded device wait timed out");
   if (st & kStatOverflow) return fail(c, PHYS_ERR_CUDA, "device workspace overflow");
   if (st & kStatNonfinite)
@@ -282,6 +285,7 @@ int phys_ctx_create(int device, phys_ctx** out) {
     char* small = nullptr;
     if ((e = cudaMalloc(&small, 4096)) != cudaSuccess) { st = cuda_fail(c, e, "cudaMalloc(small)"); break; }
     c->d_status = reinterpret_cast<int32_t*>(small);
+    // [0] interactions of the last evaluation, [1] of the group walk's list evaluation
     c->d_counter = reinterpret_cast<unsigned long long*>(small + 256);
     c->d_hdr = reinterpret_cast<TreeHeader*>(small + 512);
     if ((e = cudaMemset(small, 0, 4096)) != cudaSuccess) { st = cuda_fail(c, e, "cudaMemset"); break; }
@@ -617,6 +621,7 @@ int phys_ensemble_run(phys_ctx* c, const phys_params* p, double dt, int64_t nste
   PHYS_TRY(ensemble_run(c, p, dt, nsteps, group, chunk));
   c->tm.walk_ms = ev_ms(c->ev[6], c->ev[7]);
   c->last_eval_bh = false;
+  c->last_eval_group = false;
   int32_t sw = 0;
   PHYS_TRY(read_status(c, &sw));
   if (sw & kStatOverflow) return fail(c, PHYS_ERR_ARG, "system larger than 64 bodies");
@@ -651,6 +656,7 @@ int phys_adjoint_direct(phys_ctx* c, const phys_params* p, double dt, int64_t ns
   PHYS_TRY(adjoint(c, p, dt, nsteps, checkpoint, tx, ty, tz, loss, gxyz, gvxyz, gm));
   PHYS_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
   c->last_eval_bh = false;
+  c->last_eval_group = false;
   int st = finish_status(c);
   c->tm.total_ms = ev_ms(c->ev[0], c->ev[1]);
   return st;
@@ -663,6 +669,7 @@ int phys_trajectory_loss(phys_ctx* c, const phys_params* p, double dt, int64_t n
   PHYS_TRY(reset_status(c));
   PHYS_TRY(trajectory_loss(c, p, dt, nsteps, tx, ty, tz, loss, xT, yT, zT));
   c->last_eval_bh = false;
+  c->last_eval_group = false;
   return finish_status(c);
 }
 

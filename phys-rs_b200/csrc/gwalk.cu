@@ -748,7 +748,10 @@ geval_kernel(int n, const GNode* __restrict__ gn, const int4* __restrict__ items
       E.gather_eval(codes + b0, min(kGList, len - b0), gn, body64, B, far2);
     E.finish(body64, perm, G, want_force, ox, oy, oz, status);
   }
-  if (lane == 0 && ninter) atomicAdd(counter, ninter);  // the same on every lane
+  if (lane == 0 && ninter) {  // the same on every lane
+    atomicAdd(counter, ninter);
+    atomicAdd(counter + 1, ninter);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -907,9 +910,11 @@ int launch(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force, 
   PHYS_LAUNCH(c, glist_kernel, grid_list, kLBlock, kLSmem, (int)n, (int)t.nnodes, t.gnode,
               t.groups, t.ngroups, ctr, t.body64, theta2f, pool, pool_per_warp, items, ctr + 2,
               retry, ctr + 1, c->d_status);
+  PHYS_CUDA(c, cudaEventRecord(c->ev[10], c->stream));
   PHYS_LAUNCH(c, geval_kernel<kF32>, grid_eval, kGBlock, kESmem, (int)n, t.gnode, items, ctr + 2,
               ctr + 3, pool, t.body64, t.perm, p->G, eps2, (int)want_force, ox, oy, oz,
-              c->d_counter, c->d_status);
+              c->d_counter, c->d_status);  // adds to counter[0] and counter[1]
+  PHYS_CUDA(c, cudaEventRecord(c->ev[11], c->stream));
   PHYS_LAUNCH(c, gwalk_kernel<kF32>, grid_fused, kGBlock, kGSmem, (int)n, (int)t.nnodes, t.gnode,
               retry, ctr + 1, ctr + 4, t.body64, t.perm, p->G, eps2, theta2f, (int)want_force, ox,
               oy, oz, c->d_counter, c->d_status);

@@ -234,8 +234,9 @@ int radix_sort_u64(phys_ctx* c, uint64_t* keys, uint32_t* vals, uint64_t* keys_a
   uint32_t *vi = vals, *vo = vals_alt;
   for (int shift = begin_bit; shift < end_bit; shift += 8) {
     PHYS_LAUNCH(c, radix_hist_kernel, nblocks, kThreads, 0, ki, n, shift, nblocks, hist);
-    PHYS_LAUNCH(c, scan_single_kernel, 1, 1024, 0, hist, hist, (int64_t)kBins * nblocks,
-                (uint32_t*)nullptr);
+    // digit-major offsets: one exclusive scan over all blocks' counts
+    PHYS_TRY(scan_exclusive_i32(c, reinterpret_cast<const int32_t*>(hist),
+                                reinterpret_cast<int32_t*>(hist), (int64_t)kBins * nblocks));
     if (vals) {
       PHYS_LAUNCH(c, radix_scatter_kernel<true>, nblocks, kThreads, 0, ki, vi, ko, vo, n, shift,
                   nblocks, hist);

@@ -87,15 +87,24 @@ bbox_partial_kernel(int64_t n, const double* __restrict__ x, const double* __res
   }
 }
 
+// One warp: min/max of the partials (exact and order-free), then lane 0
+// derives the cube and the per-depth constants.
 __global__ void bbox_final_kernel(int nparts, const double* __restrict__ part, double theta,
                                   TreeHeader* hdr, const int32_t* status) {
-  if (threadIdx.x != 0) return;
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x >= 32) return;
   double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  for (int b = 0; b < nparts; ++b)
+  for (int b = lane; b < nparts; b += 32)
     for (int k = 0; k < 3; ++k) {
       mn[k] = fmin(mn[k], part[b * 6 + k]);
       mx[k] = fmax(mx[k], part[b * 6 + 3 + k]);
     }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 3; ++k) {
+      mn[k] = fmin(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+      mx[k] = fmax(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+    }
+  if (lane != 0) return;
   // extent = max - min; max_extent = x.max(y).max(z); half = max_extent*0.55 + 1
   const double ex = xsub(mx[0], mn[0]), ey = xsub(mx[1], mn[1]), ez = xsub(mx[2], mn[2]);
   const double max_extent = fmax(fmax(ex, ey), ez);

@@ -478,7 +478,7 @@ int bh_walk(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force,
   const int64_t n = t.n;
   const double eps2 = p->eps * p->eps;
   const int grid = (int)ceil_div(n, kWalkBlock);
-  PHYS_CUDA(c, cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned long long), c->stream));
+  PHYS_CUDA(c, cudaMemsetAsync(c->d_counter, 0, 2 * sizeof(unsigned long long), c->stream));
   PHYS_CUDA(c, cudaEventRecord(c->ev[6], c->stream));
   if (p->flags & PHYS_FLAG_GROUP_WALK) {
     PHYS_TRY(bh_group_walk(c, p, t, want_force, ox, oy, oz));

@@ -62,7 +62,8 @@ class Timings(ctypes.Structure):
                 ("tree_ms", ctypes.c_double), ("walk_ms", ctypes.c_double),
                 ("verlet_ms", ctypes.c_double), ("interactions", ctypes.c_uint64),
                 ("launches", ctypes.c_uint64), ("nodes", ctypes.c_int64),
-                ("max_depth", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("max_depth", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("walk_eval_ms", ctypes.c_double), ("walk_eval_interactions", ctypes.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

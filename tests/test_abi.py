@@ -4,6 +4,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 import physgpu
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -31,6 +33,29 @@ def test_status_strings_without_device():
     assert lib.phys_status_string(physgpu.ERR_NONFINITE) == b"non-finite value"
 
 
-def test_params_layout():
-    assert ctypes.sizeof(physgpu.Params) == 40
-    assert ctypes.sizeof(physgpu.Timings) == 88
+def test_params_layout(tmp_path):
+    """The ctypes mirrors match include/physgpu.h field by field (offsets
+    printed by a C program compiled against the header)."""
+    import os
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "physgpu.h"', "int main(void) {"]
+    for cname, cls in (("phys_params", physgpu.Params), ("phys_timings", physgpu.Timings)):
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
+        for f, _ in cls._fields_:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (cname, f, cname, f))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", inc, str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, cls in (("phys_params", physgpu.Params), ("phys_timings", physgpu.Timings)):
+        assert got[(cname, "size")] == ctypes.sizeof(cls)
+        for f, _ in cls._fields_:
+            assert got[(cname, f)] == getattr(cls, f).offset, (cname, f)
