@@ -4,7 +4,9 @@ Workload (default): N = 2^20 equal-mass Plummer sphere (a = 1, G = 1, seed =
 rank), theta = 0.5, eps = 0.01, dt = 1e-3, leaf capacity 8, FP32-compensated
 pair terms with FP64 state.  One step = one Velocity-Verlet tick on the device:
 bounding cube, descent keys, radix sort, octree + centre of mass, theta walk,
-kick/drift.
+kick/drift.  The walk is the group walk (one interaction list per cell group of
+at most 64 bodies); --walk body times the per-body walk, and the other walk is
+timed beside the default one in the JSON line.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -196,16 +198,18 @@ def workload_config(args, precision, leaf_cap, walk="body"):
             "l2": "flushed between timed steps (256 MiB write)"}
 
 
-# DRAM bytes (read + write) of one walk launch for the default workload
-# (N = 2^20 Plummer, theta 0.5, leaf capacity 8, F32C), from one ncu capture
-# of this binary: dram__bytes_read.sum 131.8 MB + dram__bytes_write.sum 25.3 MB.
-WALK_TRAFFIC_BYTES = 157.05e6
+# DRAM bytes (read + write) of one launch of the dominant kernel for the
+# default workload (N = 2^20 Plummer, theta 0.5, leaf capacity 8, F32C), each
+# from one ncu capture of this binary at full size:
+#   group walk, geval_kernel<true>: dram__bytes_read.sum 463.9 MB +
+#     dram__bytes_write.sum 50.4 MB;
+#   per-body walk, walk2_kernel: 131.8 MB + 25.3 MB.
+WALK_TRAFFIC_BYTES = {"group": 514.31e6, "body": 157.05e6}
 
 
 def walk_traffic(args):
-    if (args.workload, args.n, args.theta, args.leaf_cap, args.walk) == (
-            "bh", 1 << 20, 0.5, 8, "body"):
-        return WALK_TRAFFIC_BYTES
+    if (args.workload, args.n, args.theta, args.leaf_cap) == ("bh", 1 << 20, 0.5, 8):
+        return WALK_TRAFFIC_BYTES[args.walk]
     return None
 
 
@@ -381,6 +385,7 @@ def run_ours(args, ws, rank, local):
             extras["%s_walk_%s_walk_ms" % (other, name)] = statistics.median(wo)
             extras["%s_walk_%s_interactions" % (other, name)] = statistics.median(io)
             if prec == F32C:
+                ctx.upload(pos, vel, m)  # the direct sum above is at the initial positions
                 ao = ctx.gravity_accel(po)
                 e = np.linalg.norm(ao[sub] - ad, axis=1) / np.linalg.norm(ad, axis=1)
                 extras["accel_err_%s_walk_f32c_vs_f64_direct_subsample" % other] = {
