@@ -136,13 +136,13 @@ inline Status upload(Context& ctx, const World& w, const UniverseConfig& cfg, bo
 }
 
 inline Status gravity(World& w, const UniverseConfig& cfg, Context& ctx, int32_t method,
-                      Precision prec, int32_t leaf_cap) {
+                      Precision prec, int32_t leaf_cap, int32_t flags = 0) {
   if (w.size() < 2) return {};  // gravity.rs:49-51
   const bool bh = method == PHYS_BARNES_HUT;
   Status st = upload(ctx, w, cfg, bh);
   if (!st.ok()) return st;
   phys_params p{cfg.gravitational_constant, cfg.softening_epsilon, cfg.barnes_hut_theta,
-                method, (int32_t)prec, leaf_cap, 0};
+                method, (int32_t)prec, leaf_cap, flags};
   const size_t n = w.size();
   std::vector<double> fx(n), fy(n), fz(n);
   for (size_t i = 0; i < n; ++i) {
@@ -201,11 +201,14 @@ inline Status brute_force_gravity_system(World& w, const UniverseConfig& cfg, Co
   return detail::gravity(w, cfg, ctx, PHYS_DIRECT, prec, 1);
 }
 
-// src/physics/gravity_tree.rs:260-338: Force += Barnes-Hut.
+// src/physics/gravity_tree.rs:260-338: Force += Barnes-Hut.  group_walk walks
+// the tree once per cell group of at most 64 bodies (F64 / F32C only; a
+// stricter opening test, not the reference's traversal).
 inline Status barnes_hut_gravity_system(World& w, const UniverseConfig& cfg, Context& ctx,
                                         Precision prec = Precision::F64Exact,
-                                        int32_t leaf_cap = 1) {
-  return detail::gravity(w, cfg, ctx, PHYS_BARNES_HUT, prec, leaf_cap);
+                                        int32_t leaf_cap = 1, bool group_walk = false) {
+  return detail::gravity(w, cfg, ctx, PHYS_BARNES_HUT, prec, leaf_cap,
+                         group_walk ? PHYS_FLAG_GROUP_WALK : 0);
 }
 
 // src/physics/integrators.rs:110-118: a = F / m (host loop, like the
@@ -237,13 +240,13 @@ inline Status velocity_verlet_velocity_system(World& w, const SimulationTime& t,
 // LocalPosition, Velocity, Acceleration, PreviousAcceleration.
 inline Status run_velocity_verlet(World& w, const UniverseConfig& cfg, SimulationTime& t,
                                   Context& ctx, int32_t method, Precision prec,
-                                  int32_t leaf_cap, int64_t ticks) {
+                                  int32_t leaf_cap, int64_t ticks, int32_t flags = 0) {
   // positions are flattened relative to the first body's sector
   // (gravity.rs:38-47) for the whole run
   Status st = detail::upload(ctx, w, cfg, false);
   if (!st.ok()) return st;
   phys_params p{cfg.gravitational_constant, cfg.softening_epsilon, cfg.barnes_hut_theta,
-                method, (int32_t)prec, leaf_cap, 0};
+                method, (int32_t)prec, leaf_cap, flags};
   st = ctx.check(phys_verlet_steps(ctx.raw(), &p, t.dt, ticks));
   if (!st.ok()) return st;
   for (int64_t k = 0; k < ticks; ++k) t.advance_tick();

@@ -465,14 +465,14 @@ def default_context():
     return _default_ctx
 
 
-def _gravity_system(world, config, method, precision, leaf_cap, ctx, bh_quirk):
+def _gravity_system(world, config, method, precision, leaf_cap, ctx, bh_quirk, flags=0):
     ctx = ctx or default_context()
     if len(world) < 2:  # gravity.rs:49-51
         return
     ctx.upload_sectors(world.sector, world.local, config.sector_size, world.mass,
                        bh_quirk=bh_quirk)
     p = make_params(config.gravitational_constant, config.softening_epsilon,
-                    config.barnes_hut_theta, method, precision, leaf_cap)
+                    config.barnes_hut_theta, method, precision, leaf_cap, flags)
     world.force = ctx.gravity_forces(p, world.force)
 
 
@@ -481,9 +481,13 @@ def brute_force_gravity_system(world, config, precision=F64_EXACT, ctx=None):
     _gravity_system(world, config, DIRECT, precision, 1, ctx, bh_quirk=False)
 
 
-def barnes_hut_gravity_system(world, config, precision=F64_EXACT, leaf_cap=1, ctx=None):
-    """src/physics/gravity_tree.rs:260-338 on the GPU: Force += Barnes-Hut."""
-    _gravity_system(world, config, BARNES_HUT, precision, leaf_cap, ctx, bh_quirk=True)
+def barnes_hut_gravity_system(world, config, precision=F64_EXACT, leaf_cap=1, ctx=None,
+                              group_walk=False):
+    """src/physics/gravity_tree.rs:260-338 on the GPU: Force += Barnes-Hut.
+    group_walk=True walks the tree once per cell group of at most 64 bodies
+    (F64 / F32C only; stricter opening, not the reference's traversal)."""
+    _gravity_system(world, config, BARNES_HUT, precision, leaf_cap, ctx, bh_quirk=True,
+                    flags=GROUP_WALK if group_walk else 0)
 
 
 def reset_forces(world):

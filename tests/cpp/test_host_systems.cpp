@@ -122,6 +122,13 @@ static void bh_bounded_error(Context& ctx) {
   const Vec3& b = w0.force.back();
   Vec3 d{a[0] - b[0], a[1] - b[1], a[2] - b[2]};
   CHECK(norm(d) / norm(b) < 0.05, "distant body error %g", norm(d) / norm(b));
+  // the same bound through the group walk (F64, bucket leaves of 8)
+  World g5 = w5;
+  for (auto& f : g5.force) f = {0, 0, 0};
+  CHECK(barnes_hut_gravity_system(g5, c5, ctx, Precision::F64, 8, true).ok(), "group 0.5");
+  const Vec3& g = g5.force.back();
+  Vec3 dg{g[0] - b[0], g[1] - b[1], g[2] - b[2]};
+  CHECK(norm(dg) / norm(b) < 0.05, "group walk distant body error %g", norm(dg) / norm(b));
 }
 
 // integrators.rs:288-348 (300 ticks of the 6283-tick orbit, same per-tick bound)

@@ -137,3 +137,19 @@ def test_flag_rejected_outside_bh_f64_f32c(ctx, method, precision):
     assert ei.value.status == physgpu.ERR_ARG
     with pytest.raises(physgpu.PhysError):
         ctx.gravity_forces(make_params(1.0, 0.01, 0.5, BARNES_HUT, F64, 1, 2))
+
+
+def test_mirror_system_group_walk_theta_zero(ctx):
+    """barnes_hut_gravity_system(group_walk=True) at theta = 0 adds the direct
+    sum to Force (SI units, sector-flattened positions)."""
+    rng = np.random.default_rng(12)
+    wb, wd = physgpu.World(), physgpu.World()
+    for _ in range(300):
+        mm, p = 10 ** rng.uniform(20, 26), rng.normal(scale=1e9, size=3)
+        wb.spawn(mm, p)
+        wd.spawn(mm, p)
+    cfg = physgpu.UniverseConfig(softening_epsilon=1e-4, barnes_hut_theta=0.0)
+    physgpu.barnes_hut_gravity_system(wb, cfg, precision=F64, leaf_cap=8, ctx=ctx,
+                                      group_walk=True)
+    physgpu.brute_force_gravity_system(wd, cfg, precision=F64, ctx=ctx)
+    assert rel_err(wb.force, wd.force).max() < 1e-12
