@@ -168,6 +168,39 @@ int phys_gravity_accel(phys_ctx* ctx, const phys_params* p, double* ax, double* 
 int phys_direct_accel_targets(phys_ctx* ctx, const phys_params* p, int64_t nt,
                               const int64_t* targets, double* ax, double* ay, double* az);
 
+/* ---- NFW phantom halo (src/physics/nfw.rs) ------------------------------ */
+/* NfwHaloConfig (nfw.rs:24-47): rho(r) = rho_0 / ((r/Rs)(1 + r/Rs)^2),
+ * centred at `center` (local coordinates). */
+typedef struct phys_nfw_halo {
+  double rho_0;         /* central characteristic density [kg m^-3]          */
+  double scale_radius;  /* Rs [m]                                            */
+  double center[3];     /* halo centre, local coordinates [m]                */
+  int32_t enabled;      /* 0: the system and the fused term do nothing       */
+  int32_t reserved;     /* must be 0                                         */
+} phys_nfw_halo;
+
+/* nfw_density, nfw_enclosed_mass, nfw_circular_velocity (nfw.rs:61-92):
+ * host-side scalars, the reference's formulas and operation order (0 for
+ * r <= 0 or Rs <= 0; G is constants.rs:7). */
+double phys_nfw_density(double r, double rho_0, double rs);
+double phys_nfw_enclosed_mass(double r, double rho_0, double rs);
+double phys_nfw_circular_velocity(double r, double rho_0, double rs);
+
+/* nfw_gravity_system (nfw.rs:103-139) on the device: adds
+ * -G M(r) m / r^2 * r_hat to fx/fy/fz (Force +=) for every body of the
+ * context, r measured from the halo centre to the body's position as
+ * uploaded, bodies closer than 1e-10 m skipped.  G = 6.67430e-11
+ * (constants.rs:7), not phys_params.G, as in the reference.  Nothing happens
+ * when the halo is disabled. */
+int phys_nfw_forces(phys_ctx* ctx, const phys_nfw_halo* halo, double* fx, double* fy,
+                    double* fz);
+/* Makes every later acceleration of this context (phys_gravity_accel,
+ * phys_verlet_steps) include the halo the way the reference schedule does
+ * (src/main.rs:109-110,128-129: gravity, then nfw_gravity_system, then
+ * a = F/m): a = (F_gravity + F_nfw) / m.  NULL or enabled == 0 removes it.
+ * Invalidates the cached acceleration. */
+int phys_set_nfw_halo(phys_ctx* ctx, const phys_nfw_halo* halo);
+
 /* ---- integration -------------------------------------------------------- */
 /* nsteps Velocity-Verlet ticks on the device-resident state: each tick is
  * velocity_verlet_position_system (integrators.rs:63-83), a force evaluation

@@ -49,7 +49,14 @@ def lib():
         L.oracle_vv_velocity.argtypes = [i64, dbl] + [_D] * 9
         L.oracle_vv_run.argtypes = ([i64] + [_D] * 7 + [dbl, dbl, dbl, cint, dbl, i64, cint]
                                     + [_D] * 6)
+        L.oracle_vv_run_halo.argtypes = ([i64] + [_D] * 7 + [dbl, dbl, dbl, cint, dbl, i64, cint]
+                                         + [_D] * 7)
         L.oracle_energy.argtypes = [i64] + [_D] * 7 + [dbl, _D]
+        for f in ("oracle_nfw_density", "oracle_nfw_enclosed_mass",
+                  "oracle_nfw_circular_velocity"):
+            getattr(L, f).argtypes = [dbl, dbl, dbl]
+            getattr(L, f).restype = dbl
+        L.oracle_nfw_forces.argtypes = [i64] + [_D] * 4 + [_D] + [_D] * 3
         L.oracle_ensemble_run.argtypes = ([i64, _I64] + [_D] * 7 + [dbl, dbl, dbl, i64, cint]
                                           + [_D] * 3)
         _lib = L
@@ -175,8 +182,9 @@ def accel(force, m):
 
 
 def vv_run(pos, vel, m, G, eps, dt, nsteps, method="direct", theta=0.5, acc=None, prev=None,
-           nthreads=None):
-    """The reference's Velocity-Verlet tick loop (src/main.rs:103-140).
+           nthreads=None, halo=None):
+    """The reference's Velocity-Verlet tick loop (src/main.rs:103-140); `halo`
+    = (rho_0, Rs, cx, cy, cz) adds nfw_gravity_system to both force passes.
 
     Returns (pos, vel, acc, prev_acc) after `nsteps` ticks."""
     pos, vel, m = _f64(pos), _f64(vel), _f64(m)
@@ -187,9 +195,11 @@ def vv_run(pos, vel, m, G, eps, dt, nsteps, method="direct", theta=0.5, acc=None
         np.ascontiguousarray(acc[:, k], dtype=np.float64).copy() for k in range(3)]
     PA = [np.zeros(n) for _ in range(3)] if prev is None else [
         np.ascontiguousarray(prev[:, k], dtype=np.float64).copy() for k in range(3)]
-    lib().oracle_vv_run(n, *[_p(a) for a in P], *[_p(a) for a in V], _p(m), G, eps, theta,
-                        0 if method == "direct" else 1, dt, nsteps, nthreads or ncpu(),
-                        *[_p(a) for a in A], *[_p(a) for a in PA])
+    H = None if halo is None else _f64(halo)
+    lib().oracle_vv_run_halo(n, *[_p(a) for a in P], *[_p(a) for a in V], _p(m), G, eps, theta,
+                             0 if method == "direct" else 1, dt, nsteps, nthreads or ncpu(),
+                             *[_p(a) for a in A], *[_p(a) for a in PA],
+                             None if H is None else _p(H))
     st = lambda L: np.stack(L, axis=1)
     return st(P), st(V), st(A), st(PA)
 
@@ -217,3 +227,31 @@ def ensemble_run(offsets, pos, vel, m, G, eps, dt, nsteps, nthreads=None):
                               *[_p(a) for a in A])
     st = lambda L: np.stack(L, axis=1)
     return st(P), st(V), st(A)
+
+
+def nfw_density(r, rho_0, rs):
+    """nfw_density (nfw.rs:61-67)."""
+    return lib().oracle_nfw_density(float(r), float(rho_0), float(rs))
+
+
+def nfw_enclosed_mass(r, rho_0, rs):
+    """nfw_enclosed_mass (nfw.rs:76-83)."""
+    return lib().oracle_nfw_enclosed_mass(float(r), float(rho_0), float(rs))
+
+
+def nfw_circular_velocity(r, rho_0, rs):
+    """nfw_circular_velocity (nfw.rs:88-91)."""
+    return lib().oracle_nfw_circular_velocity(float(r), float(rho_0), float(rs))
+
+
+def nfw_forces(pos, m, halo, force=None):
+    """nfw_gravity_system (nfw.rs:103-139): returns force + the halo's force,
+    halo = (rho_0, Rs, cx, cy, cz)."""
+    pos, m = _f64(pos), _f64(m)
+    n = m.shape[0]
+    P = [np.ascontiguousarray(pos[:, k]) for k in range(3)]
+    F = [np.zeros(n) if force is None else np.ascontiguousarray(force[:, k], dtype=np.float64).copy()
+         for k in range(3)]
+    H = _f64(halo)
+    lib().oracle_nfw_forces(n, *[_p(a) for a in P], _p(m), _p(H), *[_p(a) for a in F])
+    return np.stack(F, axis=1)

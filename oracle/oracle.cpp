@@ -473,12 +473,58 @@ void oracle_vv_velocity(int64_t n, double dt, double* vx, double* vy, double* vz
   }
 }
 
+// nfw_density (nfw.rs:61-67)
+double oracle_nfw_density(double r, double rho_0, double rs) {
+  if (r <= 0.0 || rs <= 0.0) return 0.0;
+  const double x = r / rs;
+  const double opx = 1.0 + x;
+  return rho_0 / (x * (opx * opx));  // powi(2)
+}
+
+// nfw_enclosed_mass (nfw.rs:76-83)
+double oracle_nfw_enclosed_mass(double r, double rho_0, double rs) {
+  if (r <= 0.0 || rs <= 0.0) return 0.0;
+  const double x = r / rs;
+  const double factor = 4.0 * 3.141592653589793 * rho_0 * (rs * rs * rs);  // powi(3)
+  return factor * (std::log(1.0 + x) - x / (1.0 + x));
+}
+
+// nfw_circular_velocity (nfw.rs:88-91), G = constants.rs:7
+double oracle_nfw_circular_velocity(double r, double rho_0, double rs) {
+  const double m_enc = oracle_nfw_enclosed_mass(r, rho_0, rs);
+  return std::sqrt(std::fmax(6.67430e-11 * m_enc / r, 0.0));
+}
+
+// nfw_gravity_system (nfw.rs:103-139): Force += -r_hat * (G M(r) m / r^2)
+// for every body at r >= 1e-10 from the centre.  halo = {rho_0, Rs, cx, cy, cz}.
+void oracle_nfw_forces(int64_t n, const double* x, const double* y, const double* z,
+                       const double* m, const double* halo, double* fx, double* fy,
+                       double* fz) {
+  const double rho_0 = halo[0], rs = halo[1];
+  const V3 c = v3(halo[2], halo[3], halo[4]);
+  for (int64_t i = 0; i < n; ++i) {
+    const V3 rv = sub(v3(x[i], y[i], z[i]), c);
+    const double r = std::sqrt(len2(rv));
+    if (r < 1e-10) continue;
+    const double m_enc = oracle_nfw_enclosed_mass(r, rho_0, rs);
+    const V3 rh = divs(rv, r);
+    const double f_mag = 6.67430e-11 * m_enc * m[i] / (r * r);
+    const V3 f = mul(v3(-rh.x, -rh.y, -rh.z), f_mag);
+    fx[i] = fx[i] + f.x;
+    fy[i] = fy[i] + f.y;
+    fz[i] = fz[i] + f.z;
+  }
+}
+
+}  // extern "C"
+
 // One reference force pass: reset_forces (forces.rs:15-19), the gravity system
-// (method 0 direct, 1 Barnes-Hut), compute_acceleration_system.
+// (method 0 direct, 1 Barnes-Hut), nfw_gravity_system when `halo` is given
+// (src/main.rs:109-110), compute_acceleration_system.
 static void force_pass(int64_t n, const double* x, const double* y, const double* z,
                        const double* m, double g, double eps, double theta, int method,
                        int nthreads, double* fx, double* fy, double* fz, double* ax, double* ay,
-                       double* az) {
+                       double* az, const double* halo) {
   for (int64_t i = 0; i < n; ++i) fx[i] = fy[i] = fz[i] = 0.0;
   std::vector<double> gx(n, 0.0), gy(n, 0.0), gz(n, 0.0);
   if (method == 0)
@@ -491,25 +537,39 @@ static void force_pass(int64_t n, const double* x, const double* y, const double
     fy[i] = fy[i] + gy[i];
     fz[i] = fz[i] + gz[i];
   }
+  if (halo) oracle_nfw_forces(n, x, y, z, m, halo, fx, fy, fz);
   oracle_accel(n, fx, fy, fz, m, ax, ay, az);
 }
+
+extern "C" {
 
 // The reference's Velocity-Verlet tick (src/main.rs:103-140), `nsteps` times:
 // chain 1 = force pass, position step; chain 2 = force pass, velocity step.
 // a/pa arrays hold Acceleration / PreviousAcceleration in and out.
+// `halo` (NULL or {rho_0, Rs, cx, cy, cz}) adds nfw_gravity_system to both
+// force passes.
+void oracle_vv_run_halo(int64_t n, double* x, double* y, double* z, double* vx, double* vy,
+                        double* vz, const double* m, double g, double eps, double theta,
+                        int method, double dt, int64_t nsteps, int nthreads, double* ax,
+                        double* ay, double* az, double* pax, double* pay, double* paz,
+                        const double* halo) {
+  std::vector<double> fx(n), fy(n), fz(n);
+  for (int64_t s = 0; s < nsteps; ++s) {
+    force_pass(n, x, y, z, m, g, eps, theta, method, nthreads, fx.data(), fy.data(), fz.data(),
+               ax, ay, az, halo);
+    oracle_vv_position(n, dt, x, y, z, vx, vy, vz, ax, ay, az, pax, pay, paz);
+    force_pass(n, x, y, z, m, g, eps, theta, method, nthreads, fx.data(), fy.data(), fz.data(),
+               ax, ay, az, halo);
+    oracle_vv_velocity(n, dt, vx, vy, vz, ax, ay, az, pax, pay, paz);
+  }
+}
+
 void oracle_vv_run(int64_t n, double* x, double* y, double* z, double* vx, double* vy,
                    double* vz, const double* m, double g, double eps, double theta, int method,
                    double dt, int64_t nsteps, int nthreads, double* ax, double* ay, double* az,
                    double* pax, double* pay, double* paz) {
-  std::vector<double> fx(n), fy(n), fz(n);
-  for (int64_t s = 0; s < nsteps; ++s) {
-    force_pass(n, x, y, z, m, g, eps, theta, method, nthreads, fx.data(), fy.data(), fz.data(),
-               ax, ay, az);
-    oracle_vv_position(n, dt, x, y, z, vx, vy, vz, ax, ay, az, pax, pay, paz);
-    force_pass(n, x, y, z, m, g, eps, theta, method, nthreads, fx.data(), fy.data(), fz.data(),
-               ax, ay, az);
-    oracle_vv_velocity(n, dt, vx, vy, vz, ax, ay, az, pax, pay, paz);
-  }
+  oracle_vv_run_halo(n, x, y, z, vx, vy, vz, m, g, eps, theta, method, dt, nsteps, nthreads, ax,
+                     ay, az, pax, pay, paz, nullptr);
 }
 
 // compute_kinetic_energy_system (energy.rs:21-30), compute_potential_energy_system

@@ -58,6 +58,8 @@ struct phys_ctx {
   double *pax = nullptr, *pay = nullptr, *paz = nullptr;  // PreviousAcceleration
   double *fx = nullptr, *fy = nullptr, *fz = nullptr;     // gravity force scratch
   bool accel_valid = false;
+  phys_nfw_halo halo{};   // NFW phantom halo added to accelerations when halo_on
+  bool halo_on = false;
   phys_params accel_params{};
   bool last_eval_bh = false;   // the interaction count lives in d_counter
   bool last_eval_group = false;  // ev[10], ev[11] bracket the group walk's list evaluation
@@ -118,6 +120,10 @@ enum WsSlot {
 };
 
 // ---- kernels' host launchers (per .cu file) ----
+// nfw.cu
+int nfw_add_forces(phys_ctx* c, const phys_nfw_halo& halo, double* fx, double* fy, double* fz);
+int nfw_accel(phys_ctx* c, const phys_nfw_halo& halo, const double* fx, const double* fy,
+              const double* fz, double* ax, double* ay, double* az);
 // direct.cu
 int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, double* oy,
                 double* oz);

@@ -155,9 +155,9 @@ bool same_params(const phys_params& a, const phys_params& b) {
          a.precision == b.precision && a.leaf_cap == b.leaf_cap && a.flags == b.flags;
 }
 
-// One force evaluation on the device: accelerations into c->ax.. (want_force
-// false) or forces into c->fx.. (want_force true).
-int eval(phys_ctx* c, const phys_params* p, bool want_force) {
+// One gravity evaluation on the device: accelerations into c->ax..
+// (want_force false) or forces into c->fx.. (want_force true).
+int eval_gravity(phys_ctx* c, const phys_params* p, bool want_force) {
   double* ox = want_force ? c->fx : c->ax;
   double* oy = want_force ? c->fy : c->ay;
   double* oz = want_force ? c->fz : c->az;
@@ -172,6 +172,15 @@ int eval(phys_ctx* c, const phys_params* p, bool want_force) {
   c->last_eval_group = c->last_eval_bh && (p->flags & PHYS_FLAG_GROUP_WALK);
   if (p->method == PHYS_DIRECT) return direct_eval(c, p, want_force, ox, oy, oz);
   return bh_eval(c, p, want_force, ox, oy, oz);
+}
+
+// Forces or accelerations as the reference schedule forms them: with an NFW
+// halo set, a = (F_gravity + F_nfw) / m (src/main.rs:109-110, nfw.rs:103-139,
+// integrators.rs:110-118).
+int eval(phys_ctx* c, const phys_params* p, bool want_force) {
+  if (want_force || !c->halo_on) return eval_gravity(c, p, want_force);
+  PHYS_TRY(eval_gravity(c, p, true));
+  return nfw_accel(c, c->halo, c->fx, c->fy, c->fz, c->ax, c->ay, c->az);
 }
 
 float ev_ms(cudaEvent_t a, cudaEvent_t b);
@@ -516,6 +525,45 @@ int phys_gravity_forces(phys_ctx* c, const phys_params* p, double* fx, double* f
     fy[i] += h[n + i];
     fz[i] += h[2 * n + i];
   }
+  return PHYS_OK;
+}
+
+int phys_nfw_forces(phys_ctx* c, const phys_nfw_halo* halo, double* fx, double* fy, double* fz) {
+  if (!c) return PHYS_ERR_ARG;
+  if (!halo) return fail(c, PHYS_ERR_ARG, "halo is NULL");
+  if (halo->reserved != 0) return fail(c, PHYS_ERR_ARG, "phys_nfw_halo.reserved must be 0");
+  if (!halo->enabled) return PHYS_OK;  // nfw.rs:108-110
+  if (!fx || !fy || !fz) return fail(c, PHYS_ERR_ARG, "force arrays are required");
+  const int64_t n = c->n;
+  if (n == 0) return PHYS_OK;
+  PHYS_TRY(reset_status(c));
+  PHYS_CUDA(c, cudaMemsetAsync(c->fx, 0, sizeof(double) * n, c->stream));
+  PHYS_CUDA(c, cudaMemsetAsync(c->fy, 0, sizeof(double) * n, c->stream));
+  PHYS_CUDA(c, cudaMemsetAsync(c->fz, 0, sizeof(double) * n, c->stream));
+  PHYS_TRY(nfw_add_forces(c, *halo, c->fx, c->fy, c->fz));
+  PHYS_TRY(ensure_pinned(c, sizeof(double) * 3 * n));
+  double* h = static_cast<double*>(c->h_stage);
+  PHYS_TRY(d2h(c, h, c->fx, n));
+  PHYS_TRY(d2h(c, h + n, c->fy, n));
+  PHYS_TRY(d2h(c, h + 2 * n, c->fz, n));
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->last_eval_bh = false;
+  c->last_eval_group = false;
+  PHYS_TRY(finish_status(c));
+  for (int64_t i = 0; i < n; ++i) {  // force.0 += f_vec (nfw.rs:138)
+    fx[i] += h[i];
+    fy[i] += h[n + i];
+    fz[i] += h[2 * n + i];
+  }
+  return PHYS_OK;
+}
+
+int phys_set_nfw_halo(phys_ctx* c, const phys_nfw_halo* halo) {
+  if (!c) return PHYS_ERR_ARG;
+  if (halo && halo->reserved != 0) return fail(c, PHYS_ERR_ARG, "phys_nfw_halo.reserved must be 0");
+  c->halo_on = halo && halo->enabled;
+  if (halo) c->halo = *halo;
+  c->accel_valid = false;  // a(x) changes with the halo
   return PHYS_OK;
 }
 

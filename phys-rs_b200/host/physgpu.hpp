@@ -27,6 +27,22 @@ struct UniverseConfig {
   double sector_size = 1e12;
 };
 
+// src/physics/nfw.rs:24-47 (same defaults: a Milky-Way-like halo, off)
+struct NfwHaloConfig {
+  double rho_0 = 1.4e-21;
+  double scale_radius = 6.17e20;
+  std::array<double, 3> center{0.0, 0.0, 0.0};
+  bool enabled = false;
+  phys_nfw_halo raw() const {
+    phys_nfw_halo h{};
+    h.rho_0 = rho_0;
+    h.scale_radius = scale_radius;
+    for (int k = 0; k < 3; ++k) h.center[k] = center[k];
+    h.enabled = enabled ? 1 : 0;
+    return h;
+  }
+};
+
 // src/core/time.rs:16-77
 struct SimulationTime {
   double dt = 1.0 / 60.0;
@@ -209,6 +225,28 @@ inline Status barnes_hut_gravity_system(World& w, const UniverseConfig& cfg, Con
                                         int32_t leaf_cap = 1, bool group_walk = false) {
   return detail::gravity(w, cfg, ctx, PHYS_BARNES_HUT, prec, leaf_cap,
                          group_walk ? PHYS_FLAG_GROUP_WALK : 0);
+}
+
+// src/physics/nfw.rs:103-139: Force += the NFW halo's pull, from LocalPosition
+// (the reference ignores Sector here); nothing when the halo is disabled.
+inline Status nfw_gravity_system(World& w, const NfwHaloConfig& halo, Context& ctx) {
+  if (!halo.enabled || w.size() == 0) return {};
+  detail::Soa s = detail::gather(w);
+  Status st = ctx.check(phys_state_upload(ctx.raw(), (int64_t)w.size(), s.lx.data(), s.ly.data(),
+                                          s.lz.data(), nullptr, nullptr, nullptr, w.mass.data()));
+  if (!st.ok()) return st;
+  const size_t n = w.size();
+  std::vector<double> fx(n), fy(n), fz(n);
+  for (size_t i = 0; i < n; ++i) {
+    fx[i] = w.force[i][0];
+    fy[i] = w.force[i][1];
+    fz[i] = w.force[i][2];
+  }
+  const phys_nfw_halo h = halo.raw();
+  st = ctx.check(phys_nfw_forces(ctx.raw(), &h, fx.data(), fy.data(), fz.data()));
+  if (!st.ok()) return st;
+  for (size_t i = 0; i < n; ++i) w.force[i] = {fx[i], fy[i], fz[i]};
+  return st;
 }
 
 // src/physics/integrators.rs:110-118: a = F / m (host loop, like the

@@ -41,6 +41,8 @@ EXPORTED = [
     "phys_diagnostics", "phys_bh_export", "phys_probe_peaks", "phys_direct_accel_targets",
     "phys_ensemble_load", "phys_ensemble_run", "phys_ensemble_download", "phys_ensemble_autotune",
     "phys_direct_accel_noalloc", "phys_adjoint_direct", "phys_trajectory_loss",
+    "phys_nfw_density", "phys_nfw_enclosed_mass", "phys_nfw_circular_velocity",
+    "phys_nfw_forces", "phys_set_nfw_halo",
 ]
 
 
@@ -54,6 +56,12 @@ class Params(ctypes.Structure):
     _fields_ = [("G", ctypes.c_double), ("eps", ctypes.c_double), ("theta", ctypes.c_double),
                 ("method", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("leaf_cap", ctypes.c_int32), ("flags", ctypes.c_int32)]
+
+
+class NfwHalo(ctypes.Structure):
+    _fields_ = [("rho_0", ctypes.c_double), ("scale_radius", ctypes.c_double),
+                ("center", ctypes.c_double * 3), ("enabled", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class Timings(ctypes.Structure):
@@ -122,6 +130,11 @@ def load_library(path=None):
         "phys_trajectory_loss": ([_VP, P, dbl, i64] + [_D] * 7, ctypes.c_int),
         "phys_direct_accel_noalloc": ([i64, _VP, _VP, _VP, _VP, dbl, dbl, i32, _VP, _VP, _VP, _VP,
                                        ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
+        "phys_nfw_density": ([dbl, dbl, dbl], dbl),
+        "phys_nfw_enclosed_mass": ([dbl, dbl, dbl], dbl),
+        "phys_nfw_circular_velocity": ([dbl, dbl, dbl], dbl),
+        "phys_nfw_forces": ([_VP, ctypes.POINTER(NfwHalo), _D, _D, _D], ctypes.c_int),
+        "phys_set_nfw_halo": ([_VP, ctypes.POINTER(NfwHalo)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -252,6 +265,24 @@ class Context:
         self._check(self.lib.phys_gravity_forces(self.h, ctypes.byref(params),
                                                  *[_p(a) for a in F]), "phys_gravity_forces")
         return np.stack(F, axis=1)
+
+    def nfw_forces(self, halo, force=None):
+        """nfw_gravity_system on the device: Force += the halo's force (returns
+        the updated (n,3) array).  `halo` is an NfwHaloConfig or NfwHalo."""
+        n = self.n
+        f = np.zeros((n, 3)) if force is None else np.asarray(force, np.float64)
+        F = [np.ascontiguousarray(f[:, k]) for k in range(3)]
+        h = _halo(halo)
+        self._check(self.lib.phys_nfw_forces(self.h, ctypes.byref(h), *[_p(a) for a in F]),
+                    "phys_nfw_forces")
+        return np.stack(F, axis=1)
+
+    def set_nfw_halo(self, halo):
+        """Later accelerations (gravity_accel, verlet_steps) include the halo:
+        a = (F_gravity + F_nfw) / m.  None removes it."""
+        h = None if halo is None else _halo(halo)
+        self._check(self.lib.phys_set_nfw_halo(self.h, None if h is None else ctypes.byref(h)),
+                    "phys_set_nfw_halo")
 
     def gravity_accel(self, params, download=True):
         n = self.n
@@ -400,6 +431,43 @@ class UniverseConfig:
 
 
 @dataclass
+class NfwHaloConfig:
+    """src/physics/nfw.rs:24-47 (same defaults: a Milky-Way-like halo, off)."""
+    rho_0: float = 1.4e-21
+    scale_radius: float = 6.17e20
+    center: tuple = (0.0, 0.0, 0.0)
+    enabled: bool = False
+
+
+def _halo(cfg):
+    if isinstance(cfg, NfwHalo):
+        return cfg
+    h = NfwHalo()
+    h.rho_0 = float(cfg.rho_0)
+    h.scale_radius = float(cfg.scale_radius)
+    for k in range(3):
+        h.center[k] = float(cfg.center[k])
+    h.enabled = 1 if cfg.enabled else 0
+    h.reserved = 0
+    return h
+
+
+def nfw_density(r, rho_0, rs):
+    """nfw.rs:61-67: rho_0 / ((r/Rs)(1 + r/Rs)^2); 0 for r <= 0 or Rs <= 0."""
+    return load_library().phys_nfw_density(float(r), float(rho_0), float(rs))
+
+
+def nfw_enclosed_mass(r, rho_0, rs):
+    """nfw.rs:76-83: 4 pi rho_0 Rs^3 (ln(1 + x) - x / (1 + x)), x = r/Rs."""
+    return load_library().phys_nfw_enclosed_mass(float(r), float(rho_0), float(rs))
+
+
+def nfw_circular_velocity(r, rho_0, rs):
+    """nfw.rs:88-91: sqrt(G M(r) / r), G the SI constant."""
+    return load_library().phys_nfw_circular_velocity(float(r), float(rho_0), float(rs))
+
+
+@dataclass
 class SimulationTime:
     """src/core/time.rs:16-77 (the fixed dt the integrators read)."""
     dt: float = 1.0 / 60.0
@@ -488,6 +556,17 @@ def barnes_hut_gravity_system(world, config, precision=F64_EXACT, leaf_cap=1, ct
     (F64 / F32C only; stricter opening, not the reference's traversal)."""
     _gravity_system(world, config, BARNES_HUT, precision, leaf_cap, ctx, bh_quirk=True,
                     flags=GROUP_WALK if group_walk else 0)
+
+
+def nfw_gravity_system(world, halo_config, ctx=None):
+    """src/physics/nfw.rs:103-139 on the GPU: Force += -G M(r) m / r^2 r_hat
+    about the halo centre, from LocalPosition (the reference ignores Sector
+    here); nothing when the halo is disabled."""
+    if not halo_config.enabled or len(world) == 0:
+        return
+    ctx = ctx or default_context()
+    ctx.upload(world.local, None, world.mass)
+    world.force = ctx.nfw_forces(halo_config, world.force)
 
 
 def reset_forces(world):

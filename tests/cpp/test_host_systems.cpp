@@ -187,6 +187,25 @@ static void exact_vs_oracle(Context& ctx) {
   }
 }
 
+// nfw.rs:103-139: |F| = G M(r) m / r^2 toward the centre; disabled = no-op.
+static void nfw_halo(Context& ctx) {
+  World w;
+  w.spawn(2e30, {3e20, 4e20, 0});
+  w.spawn(1e30, {0, 0, 0});  // at the centre: skipped
+  NfwHaloConfig h;
+  CHECK(nfw_gravity_system(w, h, ctx).ok(), "disabled halo");
+  CHECK(w.force[0][0] == 0.0 && w.force[0][1] == 0.0, "disabled halo changed Force");
+  h.enabled = true;
+  CHECK(nfw_gravity_system(w, h, ctx).ok(), "nfw system");
+  const double r = 5e20;
+  const double mag = 6.67430e-11 * phys_nfw_enclosed_mass(r, h.rho_0, h.scale_radius) * 2e30 /
+                     (r * r);
+  CHECK(std::fabs(w.force[0][0] + 0.6 * mag) < 1e-12 * mag &&
+            std::fabs(w.force[0][1] + 0.8 * mag) < 1e-12 * mag,
+        "halo force %g %g vs %g", w.force[0][0], w.force[0][1], mag);
+  CHECK(w.force[1][0] == 0.0 && w.force[1][1] == 0.0 && w.force[1][2] == 0.0, "centre body");
+}
+
 int main() {
   Context ctx(0);
   if (!ctx.ok()) {
@@ -200,6 +219,7 @@ int main() {
   bh_bounded_error(ctx);
   circular_orbit(ctx);
   exact_vs_oracle(ctx);
+  nfw_halo(ctx);
   std::printf("%s (%d failures)\n", failures ? "FAILED" : "ok", failures);
   return failures ? 1 : 0;
 }

@@ -152,3 +152,74 @@ def test_guard_leaf_keeps_last_body():
     g = guard[0]
     assert ex["leaf_body"][g] == 3 and ex["mass"][g] == 9.0
     assert ex["depth"][g] in (27, 28, 40)
+
+
+# ---- src/physics/nfw.rs:150-238, against the oracle and the library's host
+# scalars (the C ABI's phys_nfw_*; no GPU needed) ----
+def _nfw_impls():
+    import physgpu
+    return [("oracle", oracle.nfw_density, oracle.nfw_enclosed_mass,
+             oracle.nfw_circular_velocity),
+            ("library", physgpu.nfw_density, physgpu.nfw_enclosed_mass,
+             physgpu.nfw_circular_velocity)]
+
+
+def test_nfw_density_at_scale_radius():
+    """nfw.rs:150-162: rho(Rs) = rho_0 / 4."""
+    for name, dens, _, _ in _nfw_impls():
+        assert abs(dens(1.0, 1.0, 1.0) - 0.25) < 1e-12, name
+
+
+def test_nfw_inner_profile():
+    """nfw.rs:164-182: rho ~ 1/r for r << Rs."""
+    for name, dens, _, _ in _nfw_impls():
+        ratio = dens(0.01, 1.0, 100.0) / dens(0.02, 1.0, 100.0)
+        assert abs(ratio - 2.0) < 0.01, name
+
+
+def test_nfw_flat_rotation_curve():
+    """nfw.rs:184-213: v_c changes by < 30 % between 5, 10, 20, 50, 100 Rs."""
+    rho_0, rs = 1e-21, 1e20
+    for name, _, _, vc in _nfw_impls():
+        v = [vc(k * rs, rho_0, rs) for k in (5.0, 10.0, 20.0, 50.0, 100.0)]
+        for i in range(1, len(v)):
+            assert abs(v[i] - v[i - 1]) / v[i - 1] < 0.3, name
+        assert all(x > 0 for x in v), name
+
+
+def test_nfw_enclosed_mass_monotonic():
+    """nfw.rs:215-237."""
+    for name, _, mass, _ in _nfw_impls():
+        ms = [mass(r, 1.0, 1.0) for r in (0.1, 0.5, 1.0, 2.0, 5.0, 10.0, 100.0)]
+        assert all(b > a for a, b in zip(ms, ms[1:])), name
+
+
+def test_nfw_scalars_library_equals_oracle():
+    """The library's host scalars restate nfw.rs with the same operation
+    order as the oracle: identical results, including the r <= 0 and Rs <= 0
+    cases."""
+    import physgpu
+    rng = np.random.default_rng(3)
+    for r, rho, rs in zip(10 ** rng.uniform(-3, 3, 200), 10 ** rng.uniform(-25, 2, 200),
+                          10 ** rng.uniform(-2, 21, 200)):
+        r = r * rs
+        assert physgpu.nfw_density(r, rho, rs) == oracle.nfw_density(r, rho, rs)
+        assert physgpu.nfw_enclosed_mass(r, rho, rs) == oracle.nfw_enclosed_mass(r, rho, rs)
+        assert (physgpu.nfw_circular_velocity(r, rho, rs)
+                == oracle.nfw_circular_velocity(r, rho, rs))
+    for f in (physgpu.nfw_density, physgpu.nfw_enclosed_mass):
+        assert f(0.0, 1.0, 1.0) == 0.0 and f(-1.0, 1.0, 1.0) == 0.0 and f(1.0, 1.0, 0.0) == 0.0
+
+
+def test_nfw_oracle_force_matches_enclosed_mass():
+    """nfw_gravity_system: |F| = G M(r) m / r^2 toward the centre; a body at
+    the centre is skipped."""
+    pos = np.array([[3e20, 4e20, 0.0], [0.0, 0.0, 0.0], [1.0, 2.0, 2.0]])
+    m = np.array([2e30, 1e30, 5.0])
+    halo = (1.4e-21, 6.17e20, 0.0, 0.0, 0.0)
+    f = oracle.nfw_forces(pos, m, halo)
+    r = 5e20
+    mag = G * oracle.nfw_enclosed_mass(r, 1.4e-21, 6.17e20) * 2e30 / (r * r)
+    assert np.allclose(f[0], [-0.6 * mag, -0.8 * mag, 0.0], rtol=1e-14)
+    assert not f[1].any()
+    assert np.all(np.isfinite(f[2])) and np.linalg.norm(f[2]) > 0
