@@ -128,6 +128,25 @@ int phys_state_upload_sectors(phys_ctx* ctx, int64_t n, const int64_t* sx, const
                               const double* lz, double sector_size, int32_t bh_quirk,
                               const double* vx, const double* vy, const double* vz,
                               const double* m);
+/* Keep the (Sector, LocalPosition) components themselves on the device
+ * (src/core/coordinates.rs).  Afterwards every force pass flattens them
+ * (origin: the first body's sector for the direct sum, each body's own for
+ * Barnes-Hut, gravity_tree.rs:280-291), phys_verlet_steps integrates
+ * LocalPosition and runs sector_boundary_system (src/physics/origin.rs:16-24,
+ * normalize_position in coordinates.rs:82-103) after every velocity step, as
+ * the reference schedule does (src/main.rs:149), and the POSITION component
+ * and phys_state_download's positions are LocalPosition.  A tick in which a
+ * body changed sector costs a second force pass (the reference always runs
+ * two).  phys_state_upload / phys_state_upload_sectors leave this mode. */
+int phys_state_upload_sector_state(phys_ctx* ctx, int64_t n, const int64_t* sx,
+                                   const int64_t* sy, const int64_t* sz, const double* lx,
+                                   const double* ly, const double* lz, double sector_size,
+                                   const double* vx, const double* vy, const double* vz,
+                                   const double* m);
+/* The Sector (any of sx/sy/sz may be NULL) and LocalPosition components of a
+ * context in that mode. */
+int phys_state_download_sector_state(phys_ctx* ctx, int64_t* sx, int64_t* sy, int64_t* sz,
+                                     double* lx, double* ly, double* lz);
 /* Set the Acceleration component (the a(x_n) a Velocity-Verlet tick starts
  * from) and mark it valid for phys_verlet_steps. */
 int phys_state_set_accel(phys_ctx* ctx, const double* ax, const double* ay, const double* az);

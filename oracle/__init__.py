@@ -57,6 +57,11 @@ def lib():
             getattr(L, f).argtypes = [dbl, dbl, dbl]
             getattr(L, f).restype = dbl
         L.oracle_nfw_forces.argtypes = [i64] + [_D] * 4 + [_D] + [_D] * 3
+        L.oracle_normalize.argtypes = [i64, _I64, _I64, _I64, _D, _D, _D, dbl]
+        L.oracle_normalize.restype = cint
+        L.oracle_vv_run_sectors.argtypes = ([i64, _I64, _I64, _I64] + [_D] * 7
+                                            + [dbl, dbl, dbl, dbl, cint, dbl, i64, cint]
+                                            + [_D] * 7)
         L.oracle_ensemble_run.argtypes = ([i64, _I64] + [_D] * 7 + [dbl, dbl, dbl, i64, cint]
                                           + [_D] * 3)
         _lib = L
@@ -255,3 +260,36 @@ def nfw_forces(pos, m, halo, force=None):
     H = _f64(halo)
     lib().oracle_nfw_forces(n, *[_p(a) for a in P], _p(m), _p(H), *[_p(a) for a in F])
     return np.stack(F, axis=1)
+
+
+def normalize(sectors, local, sector_size):
+    """sector_boundary_system (origin.rs:16-24): returns (sectors, local,
+    changed) after normalize_position on every body."""
+    S = [np.ascontiguousarray(sectors[:, k], dtype=np.int64).copy() for k in range(3)]
+    L = [np.ascontiguousarray(local[:, k], dtype=np.float64).copy() for k in range(3)]
+    n = S[0].shape[0]
+    ch = lib().oracle_normalize(n, *[_p(a, _I64) for a in S], *[_p(a) for a in L],
+                                float(sector_size))
+    return np.stack(S, axis=1), np.stack(L, axis=1), bool(ch)
+
+
+def vv_run_sectors(sectors, local, vel, m, sector_size, G, eps, dt, nsteps, method="direct",
+                   theta=0.5, halo=None, nthreads=None):
+    """The reference tick loop on (Sector, LocalPosition): flatten per force
+    pass, integrate LocalPosition, sector_boundary_system after the velocity
+    step.  Returns (sectors, local, vel, acc, prev_acc)."""
+    m = _f64(m)
+    n = m.shape[0]
+    S = [np.ascontiguousarray(sectors[:, k], dtype=np.int64).copy() for k in range(3)]
+    L = [np.ascontiguousarray(local[:, k], dtype=np.float64).copy() for k in range(3)]
+    V = [np.ascontiguousarray(vel[:, k], dtype=np.float64).copy() for k in range(3)]
+    A = [np.zeros(n) for _ in range(3)]
+    PA = [np.zeros(n) for _ in range(3)]
+    H = None if halo is None else _f64(halo)
+    lib().oracle_vv_run_sectors(n, *[_p(a, _I64) for a in S], *[_p(a) for a in L],
+                                *[_p(a) for a in V], _p(m), float(sector_size), G, eps, theta,
+                                0 if method == "direct" else 1, dt, nsteps, nthreads or ncpu(),
+                                *[_p(a) for a in A], *[_p(a) for a in PA],
+                                None if H is None else _p(H))
+    st = lambda X: np.stack(X, axis=1)
+    return st(S), st(L), st(V), st(A), st(PA)

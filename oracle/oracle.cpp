@@ -524,7 +524,8 @@ void oracle_nfw_forces(int64_t n, const double* x, const double* y, const double
 static void force_pass(int64_t n, const double* x, const double* y, const double* z,
                        const double* m, double g, double eps, double theta, int method,
                        int nthreads, double* fx, double* fy, double* fz, double* ax, double* ay,
-                       double* az, const double* halo) {
+                       double* az, const double* halo, const double* hx = nullptr,
+                       const double* hy = nullptr, const double* hz = nullptr) {
   for (int64_t i = 0; i < n; ++i) fx[i] = fy[i] = fz[i] = 0.0;
   std::vector<double> gx(n, 0.0), gy(n, 0.0), gz(n, 0.0);
   if (method == 0)
@@ -537,7 +538,8 @@ static void force_pass(int64_t n, const double* x, const double* y, const double
     fy[i] = fy[i] + gy[i];
     fz[i] = fz[i] + gz[i];
   }
-  if (halo) oracle_nfw_forces(n, x, y, z, m, halo, fx, fy, fz);
+  // the halo reads LocalPosition (nfw.rs:118): hx/hy/hz when given
+  if (halo) oracle_nfw_forces(n, hx ? hx : x, hy ? hy : y, hz ? hz : z, m, halo, fx, fy, fz);
   oracle_accel(n, fx, fy, fz, m, ax, ay, az);
 }
 
@@ -561,6 +563,59 @@ void oracle_vv_run_halo(int64_t n, double* x, double* y, double* z, double* vx, 
     force_pass(n, x, y, z, m, g, eps, theta, method, nthreads, fx.data(), fy.data(), fz.data(),
                ax, ay, az, halo);
     oracle_vv_velocity(n, dt, vx, vy, vz, ax, ay, az, pax, pay, paz);
+  }
+}
+
+// Rust `f as i64`: saturating, NaN -> 0.
+static int64_t sat_i64(double v) {
+  if (v != v) return 0;
+  if (v >= 9223372036854775807.0) return INT64_MAX;
+  if (v <= -9223372036854775808.0) return INT64_MIN;
+  return (int64_t)v;
+}
+
+// sector_boundary_system (origin.rs:16-24) = normalize_position per body
+// (coordinates.rs:82-103).  Returns 1 if any body changed sector.
+int oracle_normalize(int64_t n, int64_t* sx, int64_t* sy, int64_t* sz, double* lx, double* ly,
+                     double* lz, double sector_size) {
+  int any = 0;
+  int64_t* S[3] = {sx, sy, sz};
+  double* L[3] = {lx, ly, lz};
+  for (int64_t i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) {
+      const double shift = std::round(L[k][i] / sector_size);
+      if (shift != 0.0) {
+        S[k][i] = (int64_t)((uint64_t)S[k][i] + (uint64_t)sat_i64(shift));
+        L[k][i] -= shift * sector_size;
+        any = 1;
+      }
+    }
+  return any;
+}
+
+// The reference's Velocity-Verlet tick on (Sector, LocalPosition)
+// (src/main.rs:103-150): each force pass flattens the positions
+// (gravity.rs:38-47; Barnes-Hut: each body its own origin,
+// gravity_tree.rs:280-291), the integrators update LocalPosition, and
+// sector_boundary_system runs after the velocity step.
+void oracle_vv_run_sectors(int64_t n, int64_t* sx, int64_t* sy, int64_t* sz, double* lx,
+                           double* ly, double* lz, double* vx, double* vy, double* vz,
+                           const double* m, double sector_size, double g, double eps,
+                           double theta, int method, double dt, int64_t nsteps, int nthreads,
+                           double* ax, double* ay, double* az, double* pax, double* pay,
+                           double* paz, const double* halo) {
+  std::vector<double> fx(n), fy(n), fz(n), x(n), y(n), z(n);
+  const int quirk = method == 1 ? 1 : 0;
+  for (int64_t s = 0; s < nsteps; ++s) {
+    oracle_flatten(n, sx, sy, sz, lx, ly, lz, sector_size, quirk, x.data(), y.data(), z.data());
+    force_pass(n, x.data(), y.data(), z.data(), m, g, eps, theta, method, nthreads, fx.data(),
+               fy.data(), fz.data(), ax, ay, az, halo, lx, ly, lz);
+    oracle_vv_position(n, dt, lx, ly, lz, vx, vy, vz, ax, ay, az, pax, pay, paz);
+    oracle_flatten(n, sx, sy, sz, lx, ly, lz, sector_size, quirk, x.data(), y.data(), z.data());
+    force_pass(n, x.data(), y.data(), z.data(), m, g, eps, theta, method, nthreads, fx.data(),
+               fy.data(), fz.data(), ax, ay, az, halo, lx, ly, lz);
+    oracle_vv_velocity(n, dt, vx, vy, vz, ax, ay, az, pax, pay, paz);
+    oracle_normalize(n, sx, sy, sz, lx, ly, lz, sector_size);
   }
 }
 

@@ -60,6 +60,15 @@ struct phys_ctx {
   bool accel_valid = false;
   phys_nfw_halo halo{};   // NFW phantom halo added to accelerations when halo_on
   bool halo_on = false;
+  // (Sector, LocalPosition) state kept on the device (sector_mode): sec =
+  // sx | sy | sz (int64), loc = lx | ly | lz, each sec_cap long; x/y/z then
+  // hold the flattened positions of the last force pass.
+  int32_t* d_shift = nullptr;  // device flag: a body changed sector in the last normalisation
+  bool sector_mode = false;
+  double sector_size = 0.0;
+  int64_t* sec = nullptr;
+  double* loc = nullptr;
+  int64_t sec_cap = 0;
   phys_params accel_params{};
   bool last_eval_bh = false;   // the interaction count lives in d_counter
   bool last_eval_group = false;  // ev[10], ev[11] bracket the group walk's list evaluation
@@ -120,10 +129,16 @@ enum WsSlot {
 };
 
 // ---- kernels' host launchers (per .cu file) ----
-// nfw.cu
-int nfw_add_forces(phys_ctx* c, const phys_nfw_halo& halo, double* fx, double* fy, double* fz);
-int nfw_accel(phys_ctx* c, const phys_nfw_halo& halo, const double* fx, const double* fy,
-              const double* fz, double* ax, double* ay, double* az);
+// nfw.cu (px/py/pz: the positions the halo acts on)
+int nfw_add_forces(phys_ctx* c, const phys_nfw_halo& halo, const double* px, const double* py,
+                   const double* pz, double* fx, double* fy, double* fz);
+int nfw_accel(phys_ctx* c, const phys_nfw_halo& halo, const double* px, const double* py,
+              const double* pz, const double* fx, const double* fy, const double* fz, double* ax,
+              double* ay, double* az);
+// sectors.cu
+int sector_state_alloc(phys_ctx* c, int64_t n);
+int sector_flatten(phys_ctx* c, bool bh_quirk);
+int sector_normalize(phys_ctx* c, int32_t* shifted);
 // direct.cu
 int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, double* oy,
                 double* oz);
@@ -146,6 +161,7 @@ int scan_exclusive_i32(phys_ctx* c, const int32_t* in, int32_t* out, int64_t n);
 // verlet.cu
 int verlet_drift(phys_ctx* c, double dt);
 int verlet_kick(phys_ctx* c, double dt);
+int verlet_drift_pos(phys_ctx* c, double dt, double* x, double* y, double* z);
 int verlet_kick_drift(phys_ctx* c, double dt);
 int flatten_sectors(phys_ctx* c, const int64_t* dsx, const int64_t* dsy, const int64_t* dsz,
                     const double* dlx, const double* dly, const double* dlz, double sector_size,

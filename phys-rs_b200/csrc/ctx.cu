@@ -178,10 +178,25 @@ int eval_gravity(phys_ctx* c, const phys_params* p, bool want_force) {
 // halo set, a = (F_gravity + F_nfw) / m (src/main.rs:109-110, nfw.rs:103-139,
 // integrators.rs:110-118).
 int eval(phys_ctx* c, const phys_params* p, bool want_force) {
+  // sector mode: positions flattened for this pass (the Barnes-Hut system's
+  // per-body origin for Barnes-Hut, gravity_tree.rs:280-291)
+  if (c->sector_mode) PHYS_TRY(sector_flatten(c, p->method == PHYS_BARNES_HUT));
   if (want_force || !c->halo_on) return eval_gravity(c, p, want_force);
   PHYS_TRY(eval_gravity(c, p, true));
-  return nfw_accel(c, c->halo, c->fx, c->fy, c->fz, c->ax, c->ay, c->az);
+  // the halo reads LocalPosition (nfw.rs:118)
+  const int64_t cap = c->sec_cap;
+  const double* px = c->sector_mode ? c->loc : c->x;
+  const double* py = c->sector_mode ? c->loc + cap : c->y;
+  const double* pz = c->sector_mode ? c->loc + 2 * cap : c->z;
+  return nfw_accel(c, c->halo, px, py, pz, c->fx, c->fy, c->fz, c->ax, c->ay, c->az);
 }
+
+// Positions for a call that reads c->x directly: in sector mode, flattened
+// with the direct-sum origin (gravity.rs:38-47) or the Barnes-Hut quirk.
+int positions_ready(phys_ctx* c, bool bh_quirk) {
+  return c->sector_mode ? sector_flatten(c, bh_quirk) : PHYS_OK;
+}
+
 
 float ev_ms(cudaEvent_t a, cudaEvent_t b);
 
@@ -217,6 +232,43 @@ float ev_ms(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
+// The reference tick loop on the (Sector, LocalPosition) state: position
+// step on LocalPosition, force pass, velocity step, sector_boundary_system
+// (src/main.rs:103-140,149).  a(x) of the velocity step's force pass is reused
+// by the next tick's first pass unless a body changed sector: then the
+// flattened positions (and with the Barnes-Hut quirk the positions
+// themselves) changed, and the pass is run again as the reference does.
+int verlet_steps_sectors(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps,
+                         bool sync) {
+  const int64_t cap = c->sec_cap;
+  double *lx = c->loc, *ly = c->loc + cap, *lz = c->loc + 2 * cap;
+  int32_t* h_shift = c->h_small + 16;
+  for (int64_t s = 0; s < nsteps; ++s) {
+    if (!c->accel_valid || (c->accel_params.method != -1 && !same_params(c->accel_params, *p))) {
+      PHYS_TRY(eval(c, p, false));  // chain 1 force pass
+      c->accel_valid = true;
+      c->accel_params = *p;
+    }
+    PHYS_TRY(verlet_drift_pos(c, dt, lx, ly, lz));
+    c->accel_valid = false;
+    PHYS_TRY(eval(c, p, false));  // chain 2 force pass
+    PHYS_TRY(verlet_kick(c, dt));
+    PHYS_CUDA(c, cudaMemsetAsync(c->d_shift, 0, sizeof(int32_t), c->stream));
+    PHYS_TRY(sector_normalize(c, c->d_shift));
+    PHYS_CUDA(c, cudaMemcpyAsync(h_shift, c->d_shift, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                 c->stream));
+    PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->accel_valid = *h_shift == 0;
+    c->accel_params = *p;
+  }
+  PHYS_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+  if (sync) {
+    PHYS_TRY(finish_status(c));
+    c->tm.total_ms = ev_ms(c->ev[0], c->ev[1]);
+  }
+  return PHYS_OK;
+}
+
 int verlet_steps(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, bool sync) {
   PHYS_TRY(check_params(c, p));
   if (nsteps < 0) return fail(c, PHYS_ERR_ARG, "nsteps < 0");
@@ -224,6 +276,7 @@ int verlet_steps(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, b
   if (!(dt == dt)) return fail(c, PHYS_ERR_ARG, "dt is NaN");
   PHYS_TRY(reset_status(c));
   PHYS_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+  if (c->sector_mode) return verlet_steps_sectors(c, p, dt, nsteps, sync);
   // accel_params.method == -1: the caller supplied a(x) (Acceleration
   // component), valid whatever the params.
   if (!c->accel_valid || (c->accel_params.method != -1 && !same_params(c->accel_params, *p))) {
@@ -297,6 +350,8 @@ int phys_ctx_create(int device, phys_ctx** out) {
     // [0] interactions of the last evaluation, [1] of the group walk's list evaluation
     c->d_counter = reinterpret_cast<unsigned long long*>(small + 256);
     c->d_hdr = reinterpret_cast<TreeHeader*>(small + 512);
+    c->d_shift = reinterpret_cast<int32_t*>(small + 3840);
+    static_assert(512 + sizeof(TreeHeader) <= 3840, "small device block layout");
     if ((e = cudaMemset(small, 0, 4096)) != cudaSuccess) { st = cuda_fail(c, e, "cudaMemset"); break; }
     if ((e = cudaMallocHost(&c->h_small, 4096)) != cudaSuccess) {
       st = cuda_fail(c, e, "cudaMallocHost(small)");
@@ -318,6 +373,7 @@ int phys_ctx_destroy(phys_ctx* c) {
   for (auto& b : c->ws)
     if (b.p) cudaFree(b.p);
   if (c->x) cudaFree(c->x);
+  if (c->sec) cudaFree(c->sec);
   if (c->d_status) cudaFree(c->d_status);
   if (c->d_partials) cudaFree(c->d_partials);
   if (c->h_stage) cudaFreeHost(c->h_stage);
@@ -349,6 +405,7 @@ int phys_state_upload(phys_ctx* c, int64_t n, const double* x, const double* y, 
   PHYS_CUDA(c, cudaSetDevice(c->device));
   PHYS_TRY(ensure_state(c, n));
   c->n = n;
+  c->sector_mode = false;
   c->accel_valid = false;
   if (n == 0) return PHYS_OK;
   PHYS_TRY(h2d(c, c->x, x, n));
@@ -380,6 +437,7 @@ int phys_state_upload_sectors(phys_ctx* c, int64_t n, const int64_t* sx, const i
   PHYS_CUDA(c, cudaSetDevice(c->device));
   PHYS_TRY(ensure_state(c, n));
   c->n = n;
+  c->sector_mode = false;
   c->accel_valid = false;
   if (n == 0) return PHYS_OK;
   // Stage sectors in the force scratch arrays (same size as int64) and the
@@ -408,6 +466,59 @@ int phys_state_upload_sectors(phys_ctx* c, int64_t n, const int64_t* sx, const i
   return PHYS_OK;
 }
 
+int phys_state_upload_sector_state(phys_ctx* c, int64_t n, const int64_t* sx, const int64_t* sy,
+                                   const int64_t* sz, const double* lx, const double* ly,
+                                   const double* lz, double sector_size, const double* vx,
+                                   const double* vy, const double* vz, const double* m) {
+  if (!c) return PHYS_ERR_ARG;
+  if (n < 0 || n > (int64_t(1) << 31) - 1) return fail(c, PHYS_ERR_ARG, "n out of range");
+  if (n > 0 && (!sx || !sy || !sz || !lx || !ly || !lz || !m))
+    return fail(c, PHYS_ERR_ARG, "sectors, local positions and masses are required");
+  if (!(sector_size > 0.0)) return fail(c, PHYS_ERR_ARG, "sector_size must be > 0");
+  PHYS_CUDA(c, cudaSetDevice(c->device));
+  PHYS_TRY(ensure_state(c, n));
+  PHYS_TRY(sector_state_alloc(c, n));
+  c->n = n;
+  c->sector_mode = true;
+  c->sector_size = sector_size;
+  c->accel_valid = false;
+  if (n == 0) return PHYS_OK;
+  const int64_t cap = c->sec_cap;
+  const int64_t* hs[3] = {sx, sy, sz};
+  const double* hl[3] = {lx, ly, lz};
+  for (int k = 0; k < 3; ++k) {
+    PHYS_CUDA(c, cudaMemcpyAsync(c->sec + k * cap, hs[k], 8 * n, cudaMemcpyHostToDevice,
+                                 c->stream));
+    PHYS_TRY(h2d(c, c->loc + k * cap, hl[k], n));
+  }
+  PHYS_TRY(h2d(c, c->vx, vx, n));
+  PHYS_TRY(h2d(c, c->vy, vy, n));
+  PHYS_TRY(h2d(c, c->vz, vz, n));
+  PHYS_TRY(h2d(c, c->m, m, n));
+  double* zero[6] = {c->ax, c->ay, c->az, c->pax, c->pay, c->paz};
+  for (double* d : zero) PHYS_TRY(h2d(c, d, nullptr, n));
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PHYS_OK;
+}
+
+int phys_state_download_sector_state(phys_ctx* c, int64_t* sx, int64_t* sy, int64_t* sz,
+                                     double* lx, double* ly, double* lz) {
+  if (!c) return PHYS_ERR_ARG;
+  if (!c->sector_mode) return fail(c, PHYS_ERR_STATE, "no sector state uploaded");
+  const int64_t n = c->n, cap = c->sec_cap;
+  if (n == 0) return PHYS_OK;
+  int64_t* hs[3] = {sx, sy, sz};
+  double* hl[3] = {lx, ly, lz};
+  for (int k = 0; k < 3; ++k) {
+    if (hs[k])
+      PHYS_CUDA(c, cudaMemcpyAsync(hs[k], c->sec + k * cap, 8 * n, cudaMemcpyDeviceToHost,
+                                   c->stream));
+    PHYS_TRY(d2h(c, hl[k], c->loc + k * cap, n));
+  }
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PHYS_OK;
+}
+
 int phys_state_set_accel(phys_ctx* c, const double* ax, const double* ay, const double* az) {
   if (!c) return PHYS_ERR_ARG;
   if (!ax || !ay || !az) return fail(c, PHYS_ERR_ARG, "accelerations are required");
@@ -425,9 +536,10 @@ int phys_state_download(phys_ctx* c, double* x, double* y, double* z, double* vx
   if (!c) return PHYS_ERR_ARG;
   int64_t n = c->n;
   if (n == 0) return PHYS_OK;
-  PHYS_TRY(d2h(c, x, c->x, n));
-  PHYS_TRY(d2h(c, y, c->y, n));
-  PHYS_TRY(d2h(c, z, c->z, n));
+  const int64_t cap = c->sec_cap;
+  PHYS_TRY(d2h(c, x, c->sector_mode ? c->loc : c->x, n));  // LocalPosition in sector mode
+  PHYS_TRY(d2h(c, y, c->sector_mode ? c->loc + cap : c->y, n));
+  PHYS_TRY(d2h(c, z, c->sector_mode ? c->loc + 2 * cap : c->z, n));
   PHYS_TRY(d2h(c, vx, c->vx, n));
   PHYS_TRY(d2h(c, vy, c->vy, n));
   PHYS_TRY(d2h(c, vz, c->vz, n));
@@ -440,7 +552,17 @@ int phys_state_download(phys_ctx* c, double* x, double* y, double* z, double* vx
 
 static int comp_ptrs(phys_ctx* c, int32_t comp, double** a, double** b, double** d) {
   switch (comp) {
-    case PHYS_COMP_POSITION: *a = c->x; *b = c->y; *d = c->z; return PHYS_OK;
+    case PHYS_COMP_POSITION:  // LocalPosition in sector mode
+      if (c->sector_mode) {
+        *a = c->loc;
+        *b = c->loc + c->sec_cap;
+        *d = c->loc + 2 * c->sec_cap;
+      } else {
+        *a = c->x;
+        *b = c->y;
+        *d = c->z;
+      }
+      return PHYS_OK;
     case PHYS_COMP_VELOCITY: *a = c->vx; *b = c->vy; *d = c->vz; return PHYS_OK;
     case PHYS_COMP_ACCELERATION: *a = c->ax; *b = c->ay; *d = c->az; return PHYS_OK;
     case PHYS_COMP_PREV_ACCELERATION: *a = c->pax; *b = c->pay; *d = c->paz; return PHYS_OK;
@@ -540,7 +662,10 @@ int phys_nfw_forces(phys_ctx* c, const phys_nfw_halo* halo, double* fx, double* 
   PHYS_CUDA(c, cudaMemsetAsync(c->fx, 0, sizeof(double) * n, c->stream));
   PHYS_CUDA(c, cudaMemsetAsync(c->fy, 0, sizeof(double) * n, c->stream));
   PHYS_CUDA(c, cudaMemsetAsync(c->fz, 0, sizeof(double) * n, c->stream));
-  PHYS_TRY(nfw_add_forces(c, *halo, c->fx, c->fy, c->fz));
+  const int64_t cap = c->sec_cap;  // the halo reads LocalPosition (nfw.rs:118)
+  PHYS_TRY(nfw_add_forces(c, *halo, c->sector_mode ? c->loc : c->x,
+                          c->sector_mode ? c->loc + cap : c->y,
+                          c->sector_mode ? c->loc + 2 * cap : c->z, c->fx, c->fy, c->fz));
   PHYS_TRY(ensure_pinned(c, sizeof(double) * 3 * n));
   double* h = static_cast<double*>(c->h_stage);
   PHYS_TRY(d2h(c, h, c->fx, n));
@@ -590,6 +715,7 @@ int phys_direct_accel_targets(phys_ctx* c, const phys_params* p, int64_t nt,
                               const int64_t* targets, double* ax, double* ay, double* az) {
   if (!c) return PHYS_ERR_ARG;
   PHYS_TRY(check_params(c, p));
+  PHYS_TRY(positions_ready(c, false));
   if (nt < 0 || (nt > 0 && (!targets || !ax || !ay || !az)))
     return fail(c, PHYS_ERR_ARG, "targets and outputs are required");
   if (c->n < 2 || nt == 0) {
@@ -628,6 +754,7 @@ int phys_verlet_steps_async(phys_ctx* c, const phys_params* p, double dt, int64_
 int phys_diagnostics(phys_ctx* c, double G, double* out5) {
   if (!c || !out5) return PHYS_ERR_ARG;
   if (c->n == 0) return fail(c, PHYS_ERR_STATE, "no body state uploaded");
+  PHYS_TRY(positions_ready(c, false));
   return diagnostics(c, G, out5);
 }
 
@@ -637,6 +764,7 @@ int phys_bh_export(phys_ctx* c, const phys_params* p, int64_t cap, int64_t* nnod
                    int64_t* perm, double* root4) {
   if (!c) return PHYS_ERR_ARG;
   PHYS_TRY(check_params(c, p));
+  PHYS_TRY(positions_ready(c, true));
   if (c->n < 2) return fail(c, PHYS_ERR_STATE, "need at least 2 bodies");
   if (cap < 0) return fail(c, PHYS_ERR_ARG, "cap < 0");
   PHYS_TRY(reset_status(c));
@@ -698,6 +826,7 @@ int phys_adjoint_direct(phys_ctx* c, const phys_params* p, double dt, int64_t ns
                         double* gvy, double* gvz, double* gm) {
   if (!c || !loss) return PHYS_ERR_ARG;
   PHYS_TRY(reset_status(c));
+  PHYS_TRY(positions_ready(c, false));
   PHYS_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
   double* gxyz[3] = {gx, gy, gz};
   double* gvxyz[3] = {gvx, gvy, gvz};
@@ -715,6 +844,7 @@ int phys_trajectory_loss(phys_ctx* c, const phys_params* p, double dt, int64_t n
                          double* xT, double* yT, double* zT) {
   if (!c || !loss) return PHYS_ERR_ARG;
   PHYS_TRY(reset_status(c));
+  PHYS_TRY(positions_ready(c, false));
   PHYS_TRY(trajectory_loss(c, p, dt, nsteps, tx, ty, tz, loss, xT, yT, zT));
   c->last_eval_bh = false;
   c->last_eval_group = false;

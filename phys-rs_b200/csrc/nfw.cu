@@ -94,17 +94,19 @@ int grid_for(int64_t n) { return (int)std::min<int64_t>(ceil_div(n, kBlock), 148
 
 }  // namespace
 
-int nfw_add_forces(phys_ctx* c, const phys_nfw_halo& halo, double* fx, double* fy, double* fz) {
+int nfw_add_forces(phys_ctx* c, const phys_nfw_halo& halo, const double* px, const double* py,
+                   const double* pz, double* fx, double* fy, double* fz) {
   if (c->n == 0) return PHYS_OK;
-  PHYS_LAUNCH(c, nfw_force_kernel, grid_for(c->n), kBlock, 0, c->n, c->x, c->y, c->z, c->m,
+  PHYS_LAUNCH(c, nfw_force_kernel, grid_for(c->n), kBlock, 0, c->n, px, py, pz, c->m,
               to_halo(halo), fx, fy, fz);
   return PHYS_OK;
 }
 
-int nfw_accel(phys_ctx* c, const phys_nfw_halo& halo, const double* fx, const double* fy,
-              const double* fz, double* ax, double* ay, double* az) {
+int nfw_accel(phys_ctx* c, const phys_nfw_halo& halo, const double* px, const double* py,
+              const double* pz, const double* fx, const double* fy, const double* fz, double* ax,
+              double* ay, double* az) {
   if (c->n == 0) return PHYS_OK;
-  PHYS_LAUNCH(c, nfw_accel_kernel, grid_for(c->n), kBlock, 0, c->n, c->x, c->y, c->z, c->m,
+  PHYS_LAUNCH(c, nfw_accel_kernel, grid_for(c->n), kBlock, 0, c->n, px, py, pz, c->m,
               to_halo(halo), fx, fy, fz, ax, ay, az, c->d_status);
   return PHYS_OK;
 }

@@ -116,9 +116,12 @@ int grid_for(int64_t n) {
 
 }  // namespace
 
-int verlet_drift(phys_ctx* c, double dt) {
-  PHYS_LAUNCH(c, drift_kernel, grid_for(c->n), kBlock, 0, c->n, dt, c->x, c->y, c->z, c->vx,
-              c->vy, c->vz, c->ax, c->ay, c->az, c->pax, c->pay, c->paz);
+int verlet_drift(phys_ctx* c, double dt) { return verlet_drift_pos(c, dt, c->x, c->y, c->z); }
+
+// The position step on the given position arrays (LocalPosition in sector mode).
+int verlet_drift_pos(phys_ctx* c, double dt, double* x, double* y, double* z) {
+  PHYS_LAUNCH(c, drift_kernel, grid_for(c->n), kBlock, 0, c->n, dt, x, y, z, c->vx, c->vy, c->vz,
+              c->ax, c->ay, c->az, c->pax, c->pay, c->paz);
   return PHYS_OK;
 }
 

@@ -273,29 +273,37 @@ inline Status velocity_verlet_velocity_system(World& w, const SimulationTime& t,
   return st;
 }
 
-// A whole Velocity-Verlet schedule (src/main.rs:103-140) of `ticks` ticks,
-// device-resident: one upload, ticks on the GPU, one download of
-// LocalPosition, Velocity, Acceleration, PreviousAcceleration.
+// A whole Velocity-Verlet schedule (src/main.rs:103-150) of `ticks` ticks,
+// device-resident: one upload of the (Sector, LocalPosition) state, ticks on
+// the GPU (flatten per force pass, LocalPosition integrated,
+// sector_boundary_system after every velocity step), one download of Sector,
+// LocalPosition, Velocity, Acceleration and PreviousAcceleration.  The first
+// tick recomputes a(x), as the schedule's first force pass does.
 inline Status run_velocity_verlet(World& w, const UniverseConfig& cfg, SimulationTime& t,
                                   Context& ctx, int32_t method, Precision prec,
                                   int32_t leaf_cap, int64_t ticks, int32_t flags = 0) {
-  // positions are flattened relative to the first body's sector
-  // (gravity.rs:38-47) for the whole run
-  Status st = detail::upload(ctx, w, cfg, false);
+  const size_t n = w.size();
+  detail::Soa s = detail::gather(w);
+  Status st = ctx.check(phys_state_upload_sector_state(
+      ctx.raw(), (int64_t)n, s.sx.data(), s.sy.data(), s.sz.data(), s.lx.data(), s.ly.data(),
+      s.lz.data(), cfg.sector_size, s.vx.data(), s.vy.data(), s.vz.data(), w.mass.data()));
   if (!st.ok()) return st;
   phys_params p{cfg.gravitational_constant, cfg.softening_epsilon, cfg.barnes_hut_theta,
                 method, (int32_t)prec, leaf_cap, flags};
   st = ctx.check(phys_verlet_steps(ctx.raw(), &p, t.dt, ticks));
   if (!st.ok()) return st;
   for (int64_t k = 0; k < ticks; ++k) t.advance_tick();
-  st = detail::read3(ctx, PHYS_COMP_POSITION, w.local);
-  if (st.ok()) st = detail::read3(ctx, PHYS_COMP_VELOCITY, w.velocity);
+  st = ctx.check(phys_state_download_sector_state(ctx.raw(), s.sx.data(), s.sy.data(),
+                                                  s.sz.data(), s.lx.data(), s.ly.data(),
+                                                  s.lz.data()));
+  if (!st.ok()) return st;
+  for (size_t i = 0; i < n; ++i) {
+    w.sector[i] = {s.sx[i], s.sy[i], s.sz[i]};
+    w.local[i] = {s.lx[i], s.ly[i], s.lz[i]};
+  }
+  st = detail::read3(ctx, PHYS_COMP_VELOCITY, w.velocity);
   if (st.ok()) st = detail::read3(ctx, PHYS_COMP_ACCELERATION, w.acceleration);
   if (st.ok()) st = detail::read3(ctx, PHYS_COMP_PREV_ACCELERATION, w.prev_acceleration);
-  if (st.ok() && !w.sector.empty()) {  // positions are now in the first body's sector frame
-    const IVec3 origin = w.sector.front();
-    for (auto& s : w.sector) s = origin;
-  }
   return st;
 }
 

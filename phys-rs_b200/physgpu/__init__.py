@@ -42,7 +42,8 @@ EXPORTED = [
     "phys_ensemble_load", "phys_ensemble_run", "phys_ensemble_download", "phys_ensemble_autotune",
     "phys_direct_accel_noalloc", "phys_adjoint_direct", "phys_trajectory_loss",
     "phys_nfw_density", "phys_nfw_enclosed_mass", "phys_nfw_circular_velocity",
-    "phys_nfw_forces", "phys_set_nfw_halo",
+    "phys_nfw_forces", "phys_set_nfw_halo", "phys_state_upload_sector_state",
+    "phys_state_download_sector_state",
 ]
 
 
@@ -135,6 +136,10 @@ def load_library(path=None):
         "phys_nfw_circular_velocity": ([dbl, dbl, dbl], dbl),
         "phys_nfw_forces": ([_VP, ctypes.POINTER(NfwHalo), _D, _D, _D], ctypes.c_int),
         "phys_set_nfw_halo": ([_VP, ctypes.POINTER(NfwHalo)], ctypes.c_int),
+        "phys_state_upload_sector_state": ([_VP, i64, _I64, _I64, _I64, _D, _D, _D, dbl]
+                                           + [_D] * 4, ctypes.c_int),
+        "phys_state_download_sector_state": ([_VP, _I64, _I64, _I64, _D, _D, _D],
+                                             ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -225,6 +230,29 @@ class Context:
         A = [_col(np.asarray(acc, np.float64), k) for k in range(3)]
         self._check(self.lib.phys_state_set_accel(self.h, *[_p(a) for a in A]),
                     "phys_state_set_accel")
+
+    def upload_sector_state(self, sectors, local, sector_size, m, vel=None):
+        """Keep (Sector, LocalPosition) on the device: later force passes
+        flatten them and Verlet runs normalise sectors every tick."""
+        m = np.ascontiguousarray(m, dtype=np.float64)
+        n = m.shape[0]
+        S = [np.ascontiguousarray(np.asarray(sectors)[:, k], dtype=np.int64) for k in range(3)]
+        L = [_col(np.asarray(local, np.float64), k) for k in range(3)]
+        V = [None] * 3 if vel is None else [_col(np.asarray(vel, np.float64), k) for k in range(3)]
+        self._check(self.lib.phys_state_upload_sector_state(
+            self.h, n, *[_p(a, _I64) for a in S], *[_p(a) for a in L], float(sector_size),
+            *[_p(a) for a in V], _p(m)), "phys_state_upload_sector_state")
+        self.n = n
+
+    def download_sector_state(self):
+        """(sectors int64 (n,3), local positions (n,3))."""
+        n = self.n
+        S = [np.empty(n, dtype=np.int64) for _ in range(3)]
+        L = [np.empty(n) for _ in range(3)]
+        self._check(self.lib.phys_state_download_sector_state(
+            self.h, *[_p(a, _I64) for a in S], *[_p(a) for a in L]),
+            "phys_state_download_sector_state")
+        return np.stack(S, axis=1), np.stack(L, axis=1)
 
     def download(self):
         n = self.n
@@ -585,6 +613,34 @@ def _state_to_ctx(world, ctx):
 def compute_acceleration_system(world, ctx=None):
     """src/physics/integrators.rs:110-118: a = F / m (IEEE division)."""
     world.acceleration = world.force / world.mass[:, None]
+
+
+def run_velocity_verlet(world, config, time, ticks, method=DIRECT, precision=F64_EXACT,
+                        leaf_cap=1, flags=0, ctx=None, halo=None):
+    """`ticks` ticks of the reference's Velocity-Verlet schedule
+    (src/main.rs:103-150: gravity [+ nfw_gravity_system], a = F/m, position
+    and velocity steps, sector_boundary_system) on the device, the World's
+    Sector and LocalPosition kept there between ticks.  One upload, one
+    download; advances `time`.  The first tick recomputes a(x) as the
+    schedule's first force pass does (the Acceleration and
+    PreviousAcceleration components are overwritten before they are read)."""
+    ctx = ctx or default_context()
+    ctx.upload_sector_state(world.sector, world.local, config.sector_size, world.mass,
+                            world.velocity)
+    p = make_params(config.gravitational_constant, config.softening_epsilon,
+                    config.barnes_hut_theta, method, precision, leaf_cap, flags)
+    if halo is not None:
+        ctx.set_nfw_halo(halo)
+    try:
+        ctx.verlet_steps(p, time.dt, ticks)
+    finally:
+        if halo is not None:
+            ctx.set_nfw_halo(None)
+    world.sector, world.local = ctx.download_sector_state()
+    _, world.velocity, world.acceleration = ctx.download()
+    world.prev_acceleration = ctx.read_component(COMP_PREV_ACCELERATION)
+    for _ in range(ticks):
+        time.advance_tick()
 
 
 def velocity_verlet_position_system(world, time, ctx=None):

@@ -206,6 +206,20 @@ static void nfw_halo(Context& ctx) {
   CHECK(w.force[1][0] == 0.0 && w.force[1][1] == 0.0 && w.force[1][2] == 0.0, "centre body");
 }
 
+// run_velocity_verlet on the resident sector state: a free body crossing a
+// sector boundary ends in the next sector (coordinates.rs:82-103).
+static void sector_crossing(Context& ctx) {
+  World w;
+  w.spawn(1.0, {0.49e12, 0, 0}, {0, 0, 0}, {1e10, 0, 0});
+  UniverseConfig cfg;  // sector_size 1e12
+  SimulationTime t = SimulationTime::with_dt(1.0);
+  CHECK(run_velocity_verlet(w, cfg, t, ctx, PHYS_DIRECT, Precision::F64Exact, 1, 2).ok(),
+        "run");
+  CHECK(w.sector[0][0] == 1 && w.sector[0][1] == 0, "sector %lld", (long long)w.sector[0][0]);
+  CHECK(w.local[0][0] == (0.49e12 + 1e10 + 1e10) - 1e12, "local %.17g", w.local[0][0]);
+  CHECK(t.tick == 2, "ticks");
+}
+
 int main() {
   Context ctx(0);
   if (!ctx.ok()) {
@@ -220,6 +234,7 @@ int main() {
   circular_orbit(ctx);
   exact_vs_oracle(ctx);
   nfw_halo(ctx);
+  sector_crossing(ctx);
   std::printf("%s (%d failures)\n", failures ? "FAILED" : "ok", failures);
   return failures ? 1 : 0;
 }

@@ -223,3 +223,18 @@ def test_nfw_oracle_force_matches_enclosed_mass():
     assert np.allclose(f[0], [-0.6 * mag, -0.8 * mag, 0.0], rtol=1e-14)
     assert not f[1].any()
     assert np.all(np.isfinite(f[2])) and np.linalg.norm(f[2]) > 0
+
+
+def test_normalize_wraps_sector_oracle():
+    """coordinates.rs:136-157: 1.2e12 -> sector 1, -1.2e12 -> sector -1, local
+    within half a sector (sector_size 1e12)."""
+    s, l, ch = oracle.normalize(np.zeros((2, 3), np.int64),
+                                np.array([[1.2e12, 0, 0], [-1.2e12, 0, 0]]), 1e12)
+    assert ch and s[0, 0] == 1 and s[1, 0] == -1
+    assert np.all(np.abs(l[:, 0]) < 0.5e12 + 1.0)
+    assert l[0, 0] == 1.2e12 - 1e12 and l[1, 0] == -1.2e12 + 1e12
+    # half-way rounds away from zero (f64::round); in range: untouched
+    s, l, ch = oracle.normalize(np.zeros((2, 3), np.int64),
+                                np.array([[0.5e12, -0.5e12, 0.4e12], [1.0, 2.0, 3.0]]), 1e12)
+    assert list(s[0]) == [1, -1, 0] and list(s[1]) == [0, 0, 0]
+    assert list(l[0]) == [-0.5e12, 0.5e12, 0.4e12]
