@@ -470,8 +470,9 @@ def _line(args, ws, metric, value, unit, ms, dtype, config, **kw):
 
 
 def run_other(args, ws, rank, local):
-    """Ensemble, direct-sum and adjoint workload shapes (one device per rank,
-    independent work per rank)."""
+    """Ensemble, direct-sum and adjoint workload shapes (one device per rank).
+    The ensemble's systems are split over the ranks (strong scaling); the
+    direct and adjoint shapes run one independent replica per rank."""
     import torch
 
     import physgpu
@@ -507,7 +508,14 @@ def run_other(args, ws, rank, local):
     clocks = Clocks(local)
     line = None
     if args.workload == "ensemble":
-        off, pos, vel, m = ics.ensemble(args.n, seed=rank)
+        # one ensemble for the whole job; its systems are split over the ranks
+        # (longest first to the least-loaded rank, by N(N-1)) with no exchange
+        import physgpu.dist as pdist
+        off_all, pos_all, vel_all, m_all = ics.ensemble(args.n, seed=0)
+        nb_all = int(off_all[-1])
+        mine = pdist.shard_systems(off_all, rank, ws)
+        off, body = pdist.subset_csr(off_all, mine)
+        pos, vel, m = pos_all[body], vel_all[body], m_all[body]
         ns = np.diff(off)
         pairs = int(np.sum(ns * (ns - 1)))
         nb = int(off[-1])
@@ -522,7 +530,7 @@ def run_other(args, ws, rank, local):
         ms = timed(lambda: ctx.ensemble_run(p, args.dt, args.ens_steps, group=best), args.steps)
         clk = clocks.stop()
         t = dist.max_over_ranks(sum(ms), device="cuda")
-        value = ws * nb * args.ens_steps * args.steps / (t * 1e-3)
+        value = nb_all * args.ens_steps * args.steps / (t * 1e-3)
         ach = 20.0 * pairs * args.ens_steps * args.steps / (sum(ms) * 1e-3) / 1e12
         cpu = None
         if rank == 0 and ws == 1:
@@ -542,7 +550,8 @@ def run_other(args, ws, rank, local):
         line = _line(args, ws, "particle-steps/s, batched ensemble of %d systems (N in [3,64]), "
                      "FP32-comp forces, FP64 state" % args.n, value, "particle-steps/s",
                      t / args.steps, "f32c",
-                     {"workload": "ensemble_%d_systems" % args.n, "bodies": nb,
+                     {"workload": "ensemble_%d_systems" % args.n, "bodies": nb_all,
+                      "systems_per_rank": "split over %d rank(s) by N(N-1), no exchange" % ws,
                       "steps_per_bench_step": args.ens_steps, "eps": args.eps, "dt": args.dt,
                       "group": best, "autotune_ms": tune,
                       "launch": "one persistent launch per run, captured in a CUDA graph",
@@ -552,7 +561,7 @@ def run_other(args, ws, rank, local):
                                "achieved": ach, "peak": max(fp32_tf, fp32x2_tf),
                                "unit": "TFLOP/s", "frac": ach / max(fp32_tf, fp32x2_tf),
                                "flops_per_interaction": 20, "traffic": None},
-                     cpu_baseline=cpu, clocks=clk,
+                     cpu_baseline=cpu, clocks=clk, scaling="strong",
                      gpu_launches=ctx.timings()["launches"] - l0)
     elif args.workload == "direct":
         pos, vel, m = ics.plummer(args.n, seed=rank)
