@@ -63,6 +63,15 @@
 #ifndef GWALK_FAR
 #define GWALK_FAR 1
 #endif
+#ifndef GEVAL_UNROLL
+#define GEVAL_UNROLL 2
+#endif
+#ifndef GLIST_MIN_BLOCKS
+#define GLIST_MIN_BLOCKS 1
+#endif
+#ifndef GEVAL_MIN_BLOCKS
+#define GEVAL_MIN_BLOCKS 4
+#endif
 #ifndef GWALK_POOL_PER_BODY
 #define GWALK_POOL_PER_BODY 128
 #endif
@@ -79,6 +88,7 @@ constexpr int kGStack = 1024;  // node ids per warp
 constexpr int kGList = 256;    // shared-memory list entries per warp, 32 bytes each
 constexpr int kGThrottle = kGStack - 8 - 7 * kMaxLevels;
 constexpr int kGFlushPairs = GWALK_FLUSH_PAIRS;
+constexpr int kEvalUnroll = GEVAL_UNROLL;  // 4-entry chunks in flight per lane
 constexpr int kGListLimit = GWALK_LIST_LIMIT;  // first-pass budget (typical lists: 3-4k)
 constexpr int kGSplit = GWALK_SPLIT;            // bodies per re-queued subgroup
 // fused kernel, per warp: stack | list | emission records (end, kind, a, olo,
@@ -418,7 +428,7 @@ struct Evaluator {
       constexpr int kQ = kGFlushPairs / 2;  // 4-entry chunks per flush
       for (int q0 = 0; q0 < nq; q0 += kQ) {
         const int q1 = min(q0 + kQ, nq);
-#pragma unroll 2
+#pragma unroll kEvalUnroll
         for (int q = q0; q < q1; ++q) {
           const float4 hx = HX[q], hy = HY[q], hz = HZ[q], mm = MM[q];
           const float4 lx = LX[q], ly = LY[q], lz = LZ[q];
@@ -498,7 +508,7 @@ struct Evaluator {
     constexpr int kQ = kGFlushPairs / 2;
     for (int q0 = 0; q0 < nq; q0 += kQ) {
       const int q1 = min(q0 + kQ, nq);
-#pragma unroll 2
+#pragma unroll kEvalUnroll
       for (int q = q0; q < q1; ++q) {
         const float4 hx = HX[q], hy = HY[q], hz = HZ[q], mm = MM[q];
         term32f(lo2(hx), lo2(hy), lo2(hz), lo2(mm), nhxa, nhya, nhza, pxa, pya, pza);
@@ -647,7 +657,7 @@ __device__ __forceinline__ bool requeue(int2 gr, int n, int2* retry, int32_t* nr
 // Items: n int4 {first body, end body, 0, list length}, then n int64 pool
 // offsets.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kLBlock)
+__global__ void __launch_bounds__(kLBlock, GLIST_MIN_BLOCKS)
 glist_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __restrict__ groups,
              const int32_t* __restrict__ ngroups_p, int32_t* __restrict__ ctr,
              const double4* __restrict__ body64, float theta2f, uint32_t* __restrict__ pool,
@@ -719,7 +729,7 @@ glist_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __rest
 // 2. evaluation of the lists
 // ---------------------------------------------------------------------------
 template <bool kF32>
-__global__ void __launch_bounds__(kGBlock, 4)
+__global__ void __launch_bounds__(kGBlock, GEVAL_MIN_BLOCKS)
 geval_kernel(int n, const GNode* __restrict__ gn, const int4* __restrict__ items,
              const int32_t* __restrict__ nitems_p, int32_t* __restrict__ ctr,
              const uint32_t* __restrict__ pool, const double4* __restrict__ body64,

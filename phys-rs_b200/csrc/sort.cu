@@ -100,16 +100,30 @@ scan_single_kernel(const uint32_t* in, uint32_t* out, int64_t count, uint32_t* t
   if (tid == 0 && total) *total = carry_s;
 }
 
+// Scatter of one 4096-key tile.  Keys are ranked per warp (match/ballot, so
+// the pass is stable), then placed in shared memory in digit order and
+// written out run by run: consecutive threads write consecutive addresses
+// of one digit's run instead of 32 scattered places per warp.
+constexpr int kScatterSmem =
+    kWarps * kBins * 4 + kTileKeys * 8 + kTileKeys * 4 + 2 * kBins * 4 + 32 * 4;
+
 template <bool kHasVals>
 __global__ void __launch_bounds__(kThreads)
 radix_scatter_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                      uint64_t* __restrict__ kout, uint32_t* __restrict__ vout, int64_t n,
                      int shift, int nblocks, const uint32_t* __restrict__ offs) {
-  __shared__ uint32_t cnt[kWarps][kBins];
+  extern __shared__ __align__(16) unsigned char ssm[];
+  uint64_t* skey = reinterpret_cast<uint64_t*>(ssm);                          // kTileKeys
+  uint32_t* sval = reinterpret_cast<uint32_t*>(ssm + kTileKeys * 8);          // kTileKeys
+  uint32_t(*cnt)[kBins] = reinterpret_cast<uint32_t(*)[kBins]>(ssm + kTileKeys * 12);
+  uint32_t* local_off = reinterpret_cast<uint32_t*>(ssm + kTileKeys * 12 + kWarps * kBins * 4);
+  uint32_t* gbase = local_off + kBins;
+  uint32_t* wsum = gbase + kBins;  // 32 entries
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int i = threadIdx.x; i < kWarps * kBins; i += kThreads) (&cnt[0][0])[i] = 0;
   __syncthreads();
-  const int64_t base = blockIdx.x * (int64_t)kTileKeys + warp * kWarpKeys;
+  const int64_t tile0 = blockIdx.x * (int64_t)kTileKeys;
+  const int64_t base = tile0 + warp * kWarpKeys;
   const unsigned lt = lanemask_lt();
   uint64_t key[kItems];
   uint32_t rank[kItems];
@@ -130,11 +144,31 @@ radix_scatter_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restric
     __syncwarp();
   }
   __syncthreads();
-  for (int d = threadIdx.x; d < kBins; d += kThreads) {
-    uint32_t run = offs[(size_t)d * nblocks + blockIdx.x];
+  // digit d (one per thread): tile-local start of its run, and where the run
+  // goes in the output
+  static_assert(kThreads == kBins, "one thread per digit");
+  {
+    const int d = threadIdx.x;
+    uint32_t tot = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) tot += cnt[w][d];
+    uint32_t inc = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    uint32_t woff = 0;
+    for (int w = 0; w < warp; ++w) woff += wsum[w];
+    const uint32_t lo = woff + inc - tot;  // exclusive over digits
+    local_off[d] = lo;
+    gbase[d] = offs[(size_t)d * nblocks + blockIdx.x] - lo;
+    uint32_t run = lo;
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) {
-      uint32_t t = cnt[w][d];
+      const uint32_t t = cnt[w][d];
       cnt[w][d] = run;
       run += t;
     }
@@ -145,10 +179,19 @@ radix_scatter_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restric
     const int64_t idx = base + r * 32 + lane;
     if (idx < n) {
       const uint32_t d = (uint32_t)(key[r] >> shift) & 0xFFu;
-      const uint32_t pos = cnt[warp][d] + rank[r];
-      kout[pos] = key[r];
-      if (kHasVals) vout[pos] = vin[idx];
+      const uint32_t lpos = cnt[warp][d] + rank[r];
+      skey[lpos] = key[r];
+      if (kHasVals) sval[lpos] = vin[idx];
     }
+  }
+  __syncthreads();
+  const int tile_n = (int)min64(kTileKeys, n - tile0);
+  for (int i = threadIdx.x; i < tile_n; i += kThreads) {
+    const uint64_t k = skey[i];
+    const uint32_t d = (uint32_t)(k >> shift) & 0xFFu;
+    const uint32_t pos = gbase[d] + (uint32_t)i;
+    kout[pos] = k;
+    if (kHasVals) vout[pos] = sval[i];
   }
 }
 
@@ -226,6 +269,14 @@ int radix_sort_u64(phys_ctx* c, uint64_t* keys, uint32_t* vals, uint64_t* keys_a
                    uint32_t* vals_alt, int64_t n, int begin_bit, int end_bit, bool* in_alt) {
   *in_alt = false;
   if (n <= 1 || end_bit <= begin_bit) return PHYS_OK;
+  static bool smem_set = false;  // per process: the kernels' attributes are fixed
+  if (!smem_set) {
+    PHYS_CUDA(c, cudaFuncSetAttribute(radix_scatter_kernel<true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, kScatterSmem));
+    PHYS_CUDA(c, cudaFuncSetAttribute(radix_scatter_kernel<false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, kScatterSmem));
+    smem_set = true;
+  }
   const int nblocks = (int)ceil_div(n, kTileKeys);
   int st = PHYS_OK;
   uint32_t* hist = (uint32_t*)ws_get(c, WS_HIST, sizeof(uint32_t) * (size_t)kBins * nblocks, &st);
@@ -238,11 +289,11 @@ int radix_sort_u64(phys_ctx* c, uint64_t* keys, uint32_t* vals, uint64_t* keys_a
     PHYS_TRY(scan_exclusive_i32(c, reinterpret_cast<const int32_t*>(hist),
                                 reinterpret_cast<int32_t*>(hist), (int64_t)kBins * nblocks));
     if (vals) {
-      PHYS_LAUNCH(c, radix_scatter_kernel<true>, nblocks, kThreads, 0, ki, vi, ko, vo, n, shift,
-                  nblocks, hist);
+      PHYS_LAUNCH(c, radix_scatter_kernel<true>, nblocks, kThreads, kScatterSmem, ki, vi, ko, vo,
+                  n, shift, nblocks, hist);
     } else {
-      PHYS_LAUNCH(c, radix_scatter_kernel<false>, nblocks, kThreads, 0, ki, vi, ko, vo, n, shift,
-                  nblocks, hist);
+      PHYS_LAUNCH(c, radix_scatter_kernel<false>, nblocks, kThreads, kScatterSmem, ki, vi, ko, vo,
+                  n, shift, nblocks, hist);
     }
     uint64_t* tk = ki;
     ki = ko;
