@@ -1,7 +1,7 @@
 // K4: stable LSD radix sort of 64-bit keys with 32-bit payloads, and
 // exclusive scans.  Each 8-bit pass is histogram -> scan -> scatter; the
 // scatter ranks keys with warp match/ballot so the pass is stable (warp w of
-// a block owns keys [w*512, w*512+512) of the block's 4096-key tile).
+// a block owns keys [w*256, w*256+256) of the block's 2048-key tile).
 #include "common.cuh"
 
 namespace phys {
@@ -9,9 +9,12 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kItems = 16;                       // rounds of 32 keys per warp
-constexpr int kTileKeys = kThreads * kItems;     // 4096 keys per block
-constexpr int kWarpKeys = 32 * kItems;           // 512 keys per warp
+#ifndef SORT_ITEMS
+#define SORT_ITEMS 8
+#endif
+constexpr int kItems = SORT_ITEMS;               // rounds of 32 keys per warp
+constexpr int kTileKeys = kThreads * kItems;     // 2048 keys per block
+constexpr int kWarpKeys = 32 * kItems;           // 256 keys per warp
 constexpr int kBins = 256;
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -100,7 +103,7 @@ scan_single_kernel(const uint32_t* in, uint32_t* out, int64_t count, uint32_t* t
   if (tid == 0 && total) *total = carry_s;
 }
 
-// Scatter of one 4096-key tile.  Keys are ranked per warp (match/ballot, so
+// Scatter of one 2048-key tile.  Keys are ranked per warp (match/ballot, so
 // the pass is stable), then placed in shared memory in digit order and
 // written out run by run: consecutive threads write consecutive addresses
 // of one digit's run instead of 32 scattered places per warp.
