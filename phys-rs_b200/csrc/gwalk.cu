@@ -24,9 +24,9 @@
 //      whose list passes kGListLimit entries (a sparse group whose box
 //      reaches a much denser region) is abandoned and re-queued as
 //      subgroups of kGSplit consecutive bodies, whose lists are far shorter;
-//   2. geval_kernel evaluates the lists: per batch of kGList entries the
-//      lanes gather the sources into shared memory, then every lane
-//      accumulates its two targets over the batch (broadcast loads);
+//   2. geval_kernel evaluates the lists: batches of kEB entries stream
+//      through shared memory (cp.async, two batches in flight), then every
+//      lane accumulates its two targets over the batch (broadcast loads);
 //   3. gwalk_kernel walks and evaluates the re-queued subgroups in one pass
 //      (list in shared memory, evaluated whenever it fills).
 // The list arithmetic is the per-body walk's: F64 = f64 FMA + rsqrt on
@@ -98,9 +98,13 @@ constexpr int kGRecOff = kGListOff + kGList * 32;
 constexpr int kGSmemWarp = kGRecOff + 5 * 32 * 4 + 32 * 32;
 constexpr int kGSmem = kGWarps * kGSmemWarp;
 constexpr int kLSmem = kLWarps * kGStack * 4;  // list kernel: stacks
-// evaluation kernel, per warp: near list (7 arrays) | far list (4 arrays)
-constexpr int kESmemWarp = kGList * 7 * 4 + kGList * 4 * 4;
+// evaluation kernel, per warp: near list (7 arrays) | far list (4 arrays) of
+// kEB entries, then two staging buffers of kEB source records
+constexpr int kEB = 128;
+constexpr int kEListBytes = kEB * 7 * 4 + kEB * 4 * 4;
+constexpr int kESmemWarp = kEListBytes + 2 * kEB * 32;
 constexpr int kESmem = kGWarps * kESmemWarp;
+static_assert(kEListBytes % 32 == 0 && kEB >= kGroupMax, "evaluation kernel layout");
 static_assert(kGroupMax == 64, "two targets per lane");
 static_assert(kGThrottle >= 7 * 32 + 7, "stack too small for batched pops");
 static_assert(kGThrottle + 7 * kMaxLevels + 1 <= kGStack, "stack bound");
@@ -114,6 +118,19 @@ __device__ __forceinline__ double4 ldg_d4(const double4* p) {
   const double2* q = reinterpret_cast<const double2*>(p);
   const double2 a = __ldg(q), b = __ldg(q + 1);
   return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// 16-byte asynchronous copy global -> shared (L2 only), its commit and wait.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 __device__ __forceinline__ int warp_incl_scan(int v, int lane) {
@@ -294,15 +311,15 @@ __device__ __forceinline__ int traverse(int lane, int base, int gend, int nnodes
 // The F32C list in shared memory is a structure of arrays (slot-consecutive
 // writes hit distinct banks; the evaluation reads four entries per 16-byte
 // load).
-template <bool kF32>
+template <bool kF32, int kL>
 struct Evaluator {
   int lane, nvalid, ia, ib;
   bool va, vb;
   bool two;  // two targets per lane (more than 32 bodies), else one
   double4 X0, ta, tb;
   double eps2;
-  float* f;        // F32C list: hx, hy, hz, m, lx, ly, lz arrays of kGList
-  float* ff;       // F32C far list: hx, hy, hz, m arrays of kGList (or null)
+  float* f;        // F32C list: hx, hy, hz, m, lx, ly, lz arrays of kL
+  float* ff;       // F32C far list: hx, hy, hz, m arrays of kL (or null)
   double4* lst64;  // F64 list
   float2 nhxa, nhya, nhza, nlxa, nlya, nlza, nhxb, nhyb, nhzb, nlxb, nlyb, nlzb;
   float2 e2;
@@ -325,7 +342,7 @@ struct Evaluator {
     tb = vb ? body64[ib] : X0;
     eps2 = eps2_;
     f = reinterpret_cast<float*>(lbase);
-    ff = f + 7 * kGList;
+    ff = f + 7 * kL;
     lst64 = reinterpret_cast<double4*>(lbase);
     float h, l;
     split_df(ta.x - X0.x, h, l); nhxa = make_float2(-h, -h); nlxa = make_float2(-l, -l);
@@ -348,14 +365,14 @@ struct Evaluator {
       float h, l;
       split_df(src.x - X0.x, h, l);
       f[slot] = h;
-      f[4 * kGList + slot] = l;
+      f[4 * kL + slot] = l;
       split_df(src.y - X0.y, h, l);
-      f[kGList + slot] = h;
-      f[5 * kGList + slot] = l;
+      f[kL + slot] = h;
+      f[5 * kL + slot] = l;
       split_df(src.z - X0.z, h, l);
-      f[2 * kGList + slot] = h;
-      f[6 * kGList + slot] = l;
-      f[3 * kGList + slot] = (float)src.w;
+      f[2 * kL + slot] = h;
+      f[6 * kL + slot] = l;
+      f[3 * kL + slot] = (float)src.w;
     } else {
       lst64[slot] = src;
     }
@@ -413,18 +430,18 @@ struct Evaluator {
       const int np = (nl + 3) & ~3;
       if (lane < np - nl) {
         const int s = nl + lane;
-        f[s] = f[kGList + s] = f[2 * kGList + s] = 1e15f;
-        f[3 * kGList + s] = f[4 * kGList + s] = f[5 * kGList + s] = f[6 * kGList + s] = 0.f;
+        f[s] = f[kL + s] = f[2 * kL + s] = 1e15f;
+        f[3 * kL + s] = f[4 * kL + s] = f[5 * kL + s] = f[6 * kL + s] = 0.f;
       }
       __syncwarp();
       const int nq = np >> 2;
       const float4* HX = reinterpret_cast<const float4*>(f);
-      const float4* HY = reinterpret_cast<const float4*>(f + kGList);
-      const float4* HZ = reinterpret_cast<const float4*>(f + 2 * kGList);
-      const float4* MM = reinterpret_cast<const float4*>(f + 3 * kGList);
-      const float4* LX = reinterpret_cast<const float4*>(f + 4 * kGList);
-      const float4* LY = reinterpret_cast<const float4*>(f + 5 * kGList);
-      const float4* LZ = reinterpret_cast<const float4*>(f + 6 * kGList);
+      const float4* HY = reinterpret_cast<const float4*>(f + kL);
+      const float4* HZ = reinterpret_cast<const float4*>(f + 2 * kL);
+      const float4* MM = reinterpret_cast<const float4*>(f + 3 * kL);
+      const float4* LX = reinterpret_cast<const float4*>(f + 4 * kL);
+      const float4* LY = reinterpret_cast<const float4*>(f + 5 * kL);
+      const float4* LZ = reinterpret_cast<const float4*>(f + 6 * kL);
       constexpr int kQ = kGFlushPairs / 2;  // 4-entry chunks per flush
       for (int q0 = 0; q0 < nq; q0 += kQ) {
         const int q1 = min(q0 + kQ, nq);
@@ -496,15 +513,15 @@ struct Evaluator {
     const int np = (nl + 3) & ~3;
     if (lane < np - nl) {
       const int s = nl + lane;
-      ff[s] = ff[kGList + s] = ff[2 * kGList + s] = 1e15f;
-      ff[3 * kGList + s] = 0.f;
+      ff[s] = ff[kL + s] = ff[2 * kL + s] = 1e15f;
+      ff[3 * kL + s] = 0.f;
     }
     __syncwarp();
     const int nq = np >> 2;
     const float4* HX = reinterpret_cast<const float4*>(ff);
-    const float4* HY = reinterpret_cast<const float4*>(ff + kGList);
-    const float4* HZ = reinterpret_cast<const float4*>(ff + 2 * kGList);
-    const float4* MM = reinterpret_cast<const float4*>(ff + 3 * kGList);
+    const float4* HY = reinterpret_cast<const float4*>(ff + kL);
+    const float4* HZ = reinterpret_cast<const float4*>(ff + 2 * kL);
+    const float4* MM = reinterpret_cast<const float4*>(ff + 3 * kL);
     constexpr int kQ = kGFlushPairs / 2;
     for (int q0 = 0; q0 < nq; q0 += kQ) {
       const int q1 = min(q0 + kQ, nq);
@@ -523,71 +540,118 @@ struct Evaluator {
     __syncwarp();
   }
 
-  // Gathers list entries [0, nb) of `codes` (warp-collective) and evaluates
-  // them.  F32C: an entry whose distance from the group's box is at least
-  // GWALK_FAR box half-diagonals b goes to the far list, whose plain f32
-  // offsets from X0 need no low parts: targets lie within 2b of X0, so the
-  // separation's error is below 2^-24 (2|r| + 4b) <= 6 * 2^-24 |r|, the
-  // size of the f32 pair term's own rounding; the rest go to the near list
-  // (double-float).
-  __device__ __forceinline__ void gather_eval(const uint32_t* __restrict__ codes, int nb,
+  // Streams list entries codes[0, len) through two staging buffers of kL
+  // source records (stage: 2 * kL double4) and evaluates each batch
+  // (warp-collective).  Lane l copies entries l, l + 32, ... of a batch with
+  // cp.async and converts the same entries, so its own copies are all it
+  // waits for; batch b + 2 is in flight while batch b is evaluated, and the
+  // entry codes are read one batch further ahead.  F32C: an entry whose
+  // distance from the group's box is at least GWALK_FAR box half-diagonals b
+  // goes to the far list, whose plain f32 offsets from X0 need no low parts
+  // (targets lie within 2b of X0, so the separation's error is below
+  // 2^-24 (2|r| + 4b) <= 6 * 2^-24 |r|, the size of the f32 pair term's own
+  // rounding); the rest go to the near list (double-float).  F64: the staged
+  // records are the list.
+  __device__ __forceinline__ void stream_eval(const uint32_t* __restrict__ codes, int len,
                                               const GNode* __restrict__ gn,
                                               const double4* __restrict__ body64, const Box& B,
-                                              float far2) {
-    if (!kF32) {
-#pragma unroll 4
-      for (int e = lane; e < nb; e += 32) {
-        const uint32_t code = codes[e];
-        const int id = (int)(code >> 1);
-        put(e, (code & 1u) ? ldg_d4(&body64[id]) : ldg_d4(&gn[id].c64));
+                                              float far2, double4* stage) {
+    constexpr int kPer = kL / 32;
+    const int nb = (len + kL - 1) / kL;
+    if (nb == 0) return;
+    uint32_t pc[kPer];  // codes of the next batch to issue (~0u: none)
+    auto load_codes = [&](int b) {
+#pragma unroll
+      for (int j = 0; j < kPer; ++j) {
+        const int e = b * kL + lane + 32 * j;
+        pc[j] = e < len ? __ldg(codes + e) : ~0u;
       }
-      eval<false>(nb);
-      return;
+    };
+    auto issue = [&](int b) {
+      double4* dst = stage + (b & 1) * kL;
+#pragma unroll
+      for (int j = 0; j < kPer; ++j) {
+        if (pc[j] != ~0u) {
+          const int id = (int)(pc[j] >> 1);
+          const double4* src = (pc[j] & 1u) ? body64 + id : &gn[id].c64;
+          double4* d = dst + lane + 32 * j;
+          cp_async16(d, src);
+          cp_async16(reinterpret_cast<char*>(d) + 16, reinterpret_cast<const char*>(src) + 16);
+        }
+      }
+      cp_async_commit();
+    };
+    load_codes(0);
+    issue(0);
+    if (nb > 1) {
+      load_codes(1);
+      issue(1);
     }
-    int nnear = 0, nfar = 0;
+    if (nb > 2) load_codes(2);
     const unsigned lt = (1u << lane) - 1u;
-#pragma unroll 2
-    for (int e0 = 0; e0 < nb; e0 += 32) {
-      const int e = e0 + lane;
-      const bool valid = e < nb;
-      double4 src = make_double4(0.0, 0.0, 0.0, 0.0);
-      if (valid) {
-        const uint32_t code = codes[e];
-        const int id = (int)(code >> 1);
-        src = (code & 1u) ? ldg_d4(&body64[id]) : ldg_d4(&gn[id].c64);
+    for (int b = 0; b < nb; ++b) {
+      if (b + 1 < nb)
+        cp_async_wait<1>();
+      else
+        cp_async_wait<0>();
+      double4* buf = stage + (b & 1) * kL;
+      const int n_b = min(kL, len - b * kL);
+      if (kF32) {
+        int nnear = 0, nfar = 0;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+          const int e = lane + 32 * j;
+          const bool valid = e < n_b;
+          const double4 src = valid ? buf[e] : X0;
+          float hx, lx, hy, ly, hz, lz;
+          split_df(src.x - X0.x, hx, lx);
+          split_df(src.y - X0.y, hy, ly);
+          split_df(src.z - X0.z, hz, lz);
+          const float dx = fmaxf(fabsf(hx - B.cx) - B.bx, 0.f);
+          const float dy = fmaxf(fabsf(hy - B.cy) - B.by, 0.f);
+          const float dz = fmaxf(fabsf(hz - B.cz) - B.bz, 0.f);
+          const bool far = valid && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) >= far2;
+          const unsigned fm = __ballot_sync(kFull, far);
+          const unsigned nm = __ballot_sync(kFull, valid && !far);
+          const float m = (float)src.w;
+          if (far) {
+            const int q = nfar + __popc(fm & lt);
+            ff[q] = hx;
+            ff[kL + q] = hy;
+            ff[2 * kL + q] = hz;
+            ff[3 * kL + q] = m;
+          } else if (valid) {
+            const int q = nnear + __popc(nm & lt);
+            f[q] = hx;
+            f[kL + q] = hy;
+            f[2 * kL + q] = hz;
+            f[3 * kL + q] = m;
+            f[4 * kL + q] = lx;
+            f[5 * kL + q] = ly;
+            f[6 * kL + q] = lz;
+          }
+          nfar += __popc(fm);
+          nnear += __popc(nm);
+        }
+        __syncwarp();  // this buffer is free: refill it with batch b + 2
+        if (b + 2 < nb) {
+          issue(b + 2);
+          if (b + 3 < nb) load_codes(b + 3);
+        }
+        if (nnear) eval<false>(nnear);
+        if (nfar) eval_far(nfar);
+      } else {
+        __syncwarp();  // every lane's copies visible
+        double4* keep = lst64;
+        lst64 = buf;
+        eval<false>(n_b);
+        lst64 = keep;
+        if (b + 2 < nb) {
+          issue(b + 2);
+          if (b + 3 < nb) load_codes(b + 3);
+        }
       }
-      float hx, lx, hy, ly, hz, lz;
-      split_df(src.x - X0.x, hx, lx);
-      split_df(src.y - X0.y, hy, ly);
-      split_df(src.z - X0.z, hz, lz);
-      const float dx = fmaxf(fabsf(hx - B.cx) - B.bx, 0.f);
-      const float dy = fmaxf(fabsf(hy - B.cy) - B.by, 0.f);
-      const float dz = fmaxf(fabsf(hz - B.cz) - B.bz, 0.f);
-      const bool far = valid && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) >= far2;
-      const unsigned fm = __ballot_sync(kFull, far);
-      const unsigned nm = __ballot_sync(kFull, valid && !far);
-      const float m = (float)src.w;
-      if (far) {
-        const int q = nfar + __popc(fm & lt);
-        ff[q] = hx;
-        ff[kGList + q] = hy;
-        ff[2 * kGList + q] = hz;
-        ff[3 * kGList + q] = m;
-      } else if (valid) {
-        const int q = nnear + __popc(nm & lt);
-        f[q] = hx;
-        f[kGList + q] = hy;
-        f[2 * kGList + q] = hz;
-        f[3 * kGList + q] = m;
-        f[4 * kGList + q] = lx;
-        f[5 * kGList + q] = ly;
-        f[6 * kGList + q] = lz;
-      }
-      nfar += __popc(fm);
-      nnear += __popc(nm);
     }
-    if (nnear) eval<false>(nnear);
-    if (nfar) eval_far(nfar);
   }
 
   // Pairs inside the group, exact, i != j.
@@ -748,14 +812,14 @@ geval_kernel(int n, const GNode* __restrict__ gn, const int4* __restrict__ items
     const int4 item = items[it];
     const uint32_t* codes = pool + offs[it];
     const int len = item.w;
-    Evaluator<kF32> E;
+    Evaluator<kF32, kEB> E;
     E.init(lane, item.x, item.y, body64, lbase, eps2);
     const Box B = group_box(E.X0, E.ta, E.tb);
     const float far2 = (float)(GWALK_FAR * GWALK_FAR) * fmaf(B.bx, B.bx, fmaf(B.by, B.by, B.bz * B.bz));
     E.self_pass();
     ninter += (unsigned long long)E.nvalid * (unsigned long long)(E.nvalid - 1 + len);
-    for (int b0 = 0; b0 < len; b0 += kGList)
-      E.gather_eval(codes + b0, min(kGList, len - b0), gn, body64, B, far2);
+    E.stream_eval(codes, len, gn, body64, B, far2,
+                  reinterpret_cast<double4*>(lbase + kEListBytes));
     E.finish(body64, perm, G, want_force, ox, oy, oz, status);
   }
   if (lane == 0 && ninter) {  // the same on every lane
@@ -797,7 +861,7 @@ gwalk_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __rest
       bad = true;
       break;
     }
-    Evaluator<kF32> E;
+    Evaluator<kF32, kGList> E;
     E.init(lane, gr.x, gr.y, body64, ws + kGListOff, eps2);
     const Box B = group_box(E.X0, E.ta, E.tb);
     E.self_pass();
