@@ -28,8 +28,10 @@ struct GroupSmem {
   double ax[kMaxSys], ay[kMaxSys], az[kMaxSys];
   double pax[kMaxSys], pay[kMaxSys], paz[kMaxSys];
   double m[kMaxSys];
-  float4 h[kMaxSys];  // x_hi, y_hi, z_hi, m (f32)
-  float4 l[kMaxSys];  // x_lo, y_lo, z_lo, 0
+  // F32C staging, structure of arrays so that a float2 load gives two
+  // consecutive bodies (slot N of an odd-N system is a massless pad far away)
+  float hx[kMaxSys], hy[kMaxSys], hz[kMaxSys], hm[kMaxSys];  // hi parts, m (f32)
+  float lx[kMaxSys], ly[kMaxSys], lz[kMaxSys];               // lo parts
 };
 
 template <int G>
@@ -43,55 +45,73 @@ __device__ __forceinline__ unsigned group_mask() {
 }
 
 __device__ __forceinline__ void split_into(GroupSmem* S, int i) {
-  float4 h, l;
-  split_df(S->x[i], h.x, l.x);
-  split_df(S->y[i], h.y, l.y);
-  split_df(S->z[i], h.z, l.z);
-  h.w = (float)S->m[i];
-  l.w = 0.f;
-  S->h[i] = h;
-  S->l[i] = l;
+  split_df(S->x[i], S->hx[i], S->lx[i]);
+  split_df(S->y[i], S->hy[i], S->ly[i]);
+  split_df(S->z[i], S->hz[i], S->lz[i]);
+  S->hm[i] = (float)S->m[i];
 }
 
-// F32C accelerations of the group's own targets, TC targets per pass.
+__device__ __forceinline__ void set_pad(GroupSmem* S, int i) {
+  S->hx[i] = S->hy[i] = S->hz[i] = 1e15f;
+  S->hm[i] = S->lx[i] = S->ly[i] = S->lz[i] = 0.f;
+}
+
+__device__ __forceinline__ float2 ld2(const float* p) {
+  return *reinterpret_cast<const float2*>(p);
+}
+
+// F32C accelerations of the group's own targets, TC targets per pass.  Two
+// sources per packed f32x2 operation (bodies j, j+1; an odd N reads the pad
+// at slot N); partial sums of 16 sources folded into a (hi, lo) accumulator
+// by two-sum.
 template <int G, int TC>
 __device__ void group_forces_f32c(GroupSmem* S, int N, int gl, double Gc, float eps2f) {
+  const float2 e2 = make_float2(eps2f, eps2f);
   for (int i0 = gl; i0 < N; i0 += G * TC) {
-    float thx[TC], thy[TC], thz[TC], tlx[TC], tly[TC], tlz[TC];
-    float hx[TC], hy[TC], hz[TC], lx[TC], ly[TC], lz[TC], px[TC], py[TC], pz[TC];
+    float2 nhx[TC], nhy[TC], nhz[TC], nlx[TC], nly[TC], nlz[TC], px[TC], py[TC], pz[TC];
+    float hx[TC], hy[TC], hz[TC], lx[TC], ly[TC], lz[TC];
     int idx[TC];
 #pragma unroll
     for (int t = 0; t < TC; ++t) {
       idx[t] = i0 + t * G;
       const int ii = idx[t] < N ? idx[t] : i0;
-      const float4 h = S->h[ii], l = S->l[ii];
-      thx[t] = h.x; thy[t] = h.y; thz[t] = h.z;
-      tlx[t] = l.x; tly[t] = l.y; tlz[t] = l.z;
-      hx[t] = hy[t] = hz[t] = lx[t] = ly[t] = lz[t] = px[t] = py[t] = pz[t] = 0.f;
+      nhx[t] = make_float2(-S->hx[ii], -S->hx[ii]);
+      nhy[t] = make_float2(-S->hy[ii], -S->hy[ii]);
+      nhz[t] = make_float2(-S->hz[ii], -S->hz[ii]);
+      nlx[t] = make_float2(-S->lx[ii], -S->lx[ii]);
+      nly[t] = make_float2(-S->ly[ii], -S->ly[ii]);
+      nlz[t] = make_float2(-S->lz[ii], -S->lz[ii]);
+      hx[t] = hy[t] = hz[t] = lx[t] = ly[t] = lz[t] = 0.f;
+      px[t] = py[t] = pz[t] = make_float2(0.f, 0.f);
     }
     for (int j0 = 0; j0 < N; j0 += 16) {
       const int j1 = min(N, j0 + 16);
-      for (int j = j0; j < j1; ++j) {
-        const float4 h = S->h[j], l = S->l[j];
+      for (int j = j0; j < j1; j += 2) {
+        const float2 sx = ld2(S->hx + j), sy = ld2(S->hy + j), sz = ld2(S->hz + j);
+        const float2 sm = ld2(S->hm + j);
+        const float2 tx = ld2(S->lx + j), ty = ld2(S->ly + j), tz = ld2(S->lz + j);
 #pragma unroll
         for (int t = 0; t < TC; ++t) {
-          const float rx = (h.x - thx[t]) + (l.x - tlx[t]);
-          const float ry = (h.y - thy[t]) + (l.y - tly[t]);
-          const float rz = (h.z - thz[t]) + (l.z - tlz[t]);
-          const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2f))));
-          const float w = j == idx[t] ? 0.f : h.w * (inv * inv * inv);
-          px[t] = fmaf(rx, w, px[t]);
-          py[t] = fmaf(ry, w, py[t]);
-          pz[t] = fmaf(rz, w, pz[t]);
+          const float2 rx = __fadd2_rn(__fadd2_rn(sx, nhx[t]), __fadd2_rn(tx, nlx[t]));
+          const float2 ry = __fadd2_rn(__fadd2_rn(sy, nhy[t]), __fadd2_rn(ty, nly[t]));
+          const float2 rz = __fadd2_rn(__fadd2_rn(sz, nhz[t]), __fadd2_rn(tz, nlz[t]));
+          const float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, e2)));
+          const float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+          float2 w = __fmul2_rn(sm, __fmul2_rn(__fmul2_rn(inv, inv), inv));
+          if (j == idx[t]) w.x = 0.f;       // self (i == j skipped, gravity.rs:56)
+          if (j + 1 == idx[t]) w.y = 0.f;
+          px[t] = __ffma2_rn(rx, w, px[t]);
+          py[t] = __ffma2_rn(ry, w, py[t]);
+          pz[t] = __ffma2_rn(rz, w, pz[t]);
         }
       }
 #pragma unroll
       for (int t = 0; t < TC; ++t) {
         float s, e;
-        two_sum(hx[t], px[t], s, e); hx[t] = s; lx[t] += e;
-        two_sum(hy[t], py[t], s, e); hy[t] = s; ly[t] += e;
-        two_sum(hz[t], pz[t], s, e); hz[t] = s; lz[t] += e;
-        px[t] = py[t] = pz[t] = 0.f;
+        two_sum(hx[t], px[t].x + px[t].y, s, e); hx[t] = s; lx[t] += e;
+        two_sum(hy[t], py[t].x + py[t].y, s, e); hy[t] = s; ly[t] += e;
+        two_sum(hz[t], pz[t].x + pz[t].y, s, e); hz[t] = s; lz[t] += e;
+        px[t] = py[t] = pz[t] = make_float2(0.f, 0.f);
       }
     }
 #pragma unroll
@@ -177,6 +197,7 @@ ensemble_kernel(int nsys, const int32_t* __restrict__ order, const int64_t* __re
       S->m[i] = m[b + i];
       split_into(S, i);
     }
+    if ((N & 1) && gl == 0) set_pad(S, N);  // N <= kMaxSys - 1 here
     __syncwarp(gm);
     if (need_accel && N >= 2) group_forces<G, kExact>(S, N, gl, Gc, eps2);
     if (need_accel && N < 2)
