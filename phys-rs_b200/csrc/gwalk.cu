@@ -33,7 +33,8 @@
 // absolute coordinates; F32C = f32 pair terms on double-float coordinates
 // relative to the group's first body, r = (hi_j - hi_i) + (lo_j - lo_i), two
 // list entries per packed f32x2 operation, partial sums folded into a
-// (hi, lo) accumulator by two-sum every kGFlushPairs entry pairs.  The
+// (hi, lo) accumulator by two-sum every kGFlushPairs entry pairs (counted
+// across the near and far lists and across staging batches).  The
 // opening decisions are made in f32 for both precisions (with a 1e-5
 // relative margin toward opening), so both evaluate the same lists.
 //
@@ -52,7 +53,7 @@
 #include "bh.cuh"
 
 #ifndef GWALK_FLUSH_PAIRS
-#define GWALK_FLUSH_PAIRS 16
+#define GWALK_FLUSH_PAIRS 32
 #endif
 #ifndef GWALK_LIST_LIMIT
 #define GWALK_LIST_LIMIT 8192
@@ -324,6 +325,7 @@ struct Evaluator {
   float2 nhxa, nhya, nhza, nlxa, nlya, nlza, nhxb, nhyb, nhzb, nlxb, nlyb, nlzb;
   float2 e2;
   float2 pxa, pya, pza, pxb, pyb, pzb;  // partials (entry halves)
+  int pend;                             // 4-entry chunks in the partials
   float2 Hx, Hy, Hz, Lx, Ly, Lz;        // (target a, target b)
   double ax, ay, az, bx, by, bz;        // F64 sums
 
@@ -357,6 +359,18 @@ struct Evaluator {
     pxa = pya = pza = pxb = pyb = pzb = z;
     Hx = Hy = Hz = Lx = Ly = Lz = z;
     ax = ay = az = bx = by = bz = 0.0;
+    pend = 0;
+  }
+
+  // The partials are folded into (H, L) every kFlushChunks chunks, across
+  // the near and far lists and across batches.
+  static constexpr int kFlushChunks = kGFlushPairs / 2;
+  __device__ __forceinline__ void chunks_done(int k) {
+    pend += k;
+    if (pend >= kFlushChunks) {
+      flush();
+      pend = 0;
+    }
   }
 
   // List slot from an absolute position + mass.
@@ -442,9 +456,8 @@ struct Evaluator {
       const float4* LX = reinterpret_cast<const float4*>(f + 4 * kL);
       const float4* LY = reinterpret_cast<const float4*>(f + 5 * kL);
       const float4* LZ = reinterpret_cast<const float4*>(f + 6 * kL);
-      constexpr int kQ = kGFlushPairs / 2;  // 4-entry chunks per flush
-      for (int q0 = 0; q0 < nq; q0 += kQ) {
-        const int q1 = min(q0 + kQ, nq);
+      for (int q0 = 0; q0 < nq;) {
+        const int q1 = min(q0 + (kFlushChunks - pend), nq);
 #pragma unroll kEvalUnroll
         for (int q = q0; q < q1; ++q) {
           const float4 hx = HX[q], hy = HY[q], hz = HZ[q], mm = MM[q];
@@ -479,7 +492,8 @@ struct Evaluator {
                    nhzb, nlxb, nlyb, nlzb, false, b1, pxb, pyb, pzb);
           }
         }
-        flush();
+        chunks_done(q1 - q0);
+        q0 = q1;
       }
     } else {
       __syncwarp();
@@ -522,9 +536,8 @@ struct Evaluator {
     const float4* HY = reinterpret_cast<const float4*>(ff + kL);
     const float4* HZ = reinterpret_cast<const float4*>(ff + 2 * kL);
     const float4* MM = reinterpret_cast<const float4*>(ff + 3 * kL);
-    constexpr int kQ = kGFlushPairs / 2;
-    for (int q0 = 0; q0 < nq; q0 += kQ) {
-      const int q1 = min(q0 + kQ, nq);
+    for (int q0 = 0; q0 < nq;) {
+      const int q1 = min(q0 + (kFlushChunks - pend), nq);
 #pragma unroll kEvalUnroll
       for (int q = q0; q < q1; ++q) {
         const float4 hx = HX[q], hy = HY[q], hz = HZ[q], mm = MM[q];
@@ -535,7 +548,8 @@ struct Evaluator {
           term32f(hi2(hx), hi2(hy), hi2(hz), hi2(mm), nhxb, nhyb, nhzb, pxb, pyb, pzb);
         }
       }
-      flush();
+      chunks_done(q1 - q0);
+      q0 = q1;
     }
     __syncwarp();
   }
@@ -678,6 +692,7 @@ struct Evaluator {
       if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz)) atomicOr(status, kStatNonfinite);
     };
     if (kF32) {
+      flush();  // the partials of the last chunks
       if (va) out(ia, (double)Hx.x + (double)Lx.x, (double)Hy.x + (double)Ly.x,
                   (double)Hz.x + (double)Lz.x);
       if (vb) out(ib, (double)Hx.y + (double)Lx.y, (double)Hy.y + (double)Ly.y,
