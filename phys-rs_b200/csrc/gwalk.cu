@@ -62,7 +62,7 @@
 #define GWALK_SPLIT 4
 #endif
 #ifndef GWALK_FAR
-#define GWALK_FAR 1
+#define GWALK_FAR 0.5
 #endif
 #ifndef GEVAL_UNROLL
 #define GEVAL_UNROLL 2
@@ -563,8 +563,9 @@ struct Evaluator {
   // distance from the group's box is at least GWALK_FAR box half-diagonals b
   // goes to the far list, whose plain f32 offsets from X0 need no low parts
   // (targets lie within 2b of X0, so the separation's error is below
-  // 2^-24 (2|r| + 4b) <= 6 * 2^-24 |r|, the size of the f32 pair term's own
-  // rounding); the rest go to the near list (double-float).  F64: the staged
+  // 2^-24 (2|r| + 4b) <= 10 * 2^-24 |r| at 0.5 half-diagonals, the size of
+  // the f32 pair term's own rounding); the rest go to the near list
+  // (double-float).  F64: the staged
   // records are the list.
   __device__ __forceinline__ void stream_eval(const uint32_t* __restrict__ codes, int len,
                                               const GNode* __restrict__ gn,
