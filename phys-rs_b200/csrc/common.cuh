@@ -230,6 +230,17 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
   e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
 }
 
+// 1/sqrt(x) straight from the SFU: PTX rsqrt.approx.ftz.f32, relative error
+// at most 2^-22.9 (the bound the PTX ISA states).  Every caller passes
+// r^2 + eps^2 or a squared distance, so subnormal inputs do not arise in
+// practice; flushing them lets the call compile to the one SFU instruction,
+// without the input range handling a non-FTZ build adds around it.
+__device__ __forceinline__ float rsqrt_sfu(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // Split a double into a float pair with hi + lo ~= v to ~2^-48 relative.
 __device__ __forceinline__ void split_df(double v, float& hi, float& lo) {
   hi = __double2float_rn(v);

@@ -183,7 +183,7 @@ __device__ __forceinline__ void f32_group(const float4* __restrict__ th,
       mj = 0.f;
       r2 = 1.f;
     }
-    const float inv = rsqrtf(r2);
+    const float inv = rsqrt_sfu(r2);
     const float w = mj * (inv * inv * inv);
     px = fmaf(rx, w, px);
     py = fmaf(ry, w, py);

@@ -96,7 +96,7 @@ __device__ void group_forces_f32c(GroupSmem* S, int N, int gl, double Gc, float 
           const float2 ry = __fadd2_rn(__fadd2_rn(sy, nhy[t]), __fadd2_rn(ty, nly[t]));
           const float2 rz = __fadd2_rn(__fadd2_rn(sz, nhz[t]), __fadd2_rn(tz, nlz[t]));
           const float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, e2)));
-          const float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+          const float2 inv = make_float2(rsqrt_sfu(r2.x), rsqrt_sfu(r2.y));
           float2 w = __fmul2_rn(sm, __fmul2_rn(__fmul2_rn(inv, inv), inv));
           if (j == idx[t]) w.x = 0.f;       // self (i == j skipped, gravity.rs:56)
           if (j + 1 == idx[t]) w.y = 0.f;

@@ -417,7 +417,7 @@ struct Evaluator {
     const float2 ry = __fadd2_rn(__fadd2_rn(hy, nhy), __fadd2_rn(ly, nly));
     const float2 rz = __fadd2_rn(__fadd2_rn(hz, nhz), __fadd2_rn(lz, nlz));
     const float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, e2)));
-    const float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 inv = make_float2(rsqrt_sfu(r2.x), rsqrt_sfu(r2.y));
     float2 w = __fmul2_rn(mm, __fmul2_rn(__fmul2_rn(inv, inv), inv));
     if (skip_e) w.x = 0.f;
     if (skip_f) w.y = 0.f;
@@ -515,7 +515,7 @@ struct Evaluator {
     const float2 ry = __fadd2_rn(hy, nhy);
     const float2 rz = __fadd2_rn(hz, nhz);
     const float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, e2)));
-    const float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 inv = make_float2(rsqrt_sfu(r2.x), rsqrt_sfu(r2.y));
     const float2 w = __fmul2_rn(mm, __fmul2_rn(__fmul2_rn(inv, inv), inv));
     px = __ffma2_rn(rx, w, px);
     py = __ffma2_rn(ry, w, py);

@@ -130,14 +130,14 @@ walk_kernel(int n, int nnodes, const Rec32* __restrict__ w32, const Rec64* __res
       const bool use = act && acc && L.y != p;
 #if WALK_BRANCHY
       if (use) {
-        const float inv = rsqrtf(d2 + eps2f);
+        const float inv = rsqrt_sfu(d2 + eps2f);
         const float w = A.w * (inv * inv * inv);
         px = fmaf(rx, w, px);
         py = fmaf(ry, w, py);
         pz = fmaf(rz, w, pz);
       }
 #else
-      const float inv = rsqrtf(d2 + eps2f);
+      const float inv = rsqrt_sfu(d2 + eps2f);
       const float w = use ? A.w * (inv * inv * inv) : 0.f;
       px = fmaf(rx, w, px);
       py = fmaf(ry, w, py);
@@ -171,7 +171,7 @@ walk_kernel(int n, int nnodes, const Rec32* __restrict__ w32, const Rec64* __res
             const float rx = (h.x - thx) + (l.x - tlx);
             const float ry = (h.y - thy) + (l.y - tly);
             const float rz = (h.z - thz) + (l.z - tlz);
-            const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2f))));
+            const float inv = rsqrt_sfu(fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2f))));
             const float w = use ? h.w * (inv * inv * inv) : 0.f;
             px = fmaf(rx, w, px);
             py = fmaf(ry, w, py);
@@ -300,7 +300,7 @@ walk2_kernel(int n, int nnodes, const Rec32x2* __restrict__ w, const Body32x2* _
     rz = __fadd2_rn(__fadd2_rn(lo2(q1), nhz), __fadd2_rn(lo2(q3), nlz));
   };
   auto accum = [&](float2 rx, float2 ry, float2 rz, float2 r2, float2 m2, bool ua, bool ub) {
-    const float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 inv = make_float2(rsqrt_sfu(r2.x), rsqrt_sfu(r2.y));
     float2 wg = __fmul2_rn(m2, __fmul2_rn(__fmul2_rn(inv, inv), inv));
     wg.x = ua ? wg.x : 0.f;
     wg.y = ub ? wg.y : 0.f;
