@@ -45,6 +45,10 @@ struct TreeHeader {
 struct phys_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // second stream for work that runs beside the main stream's kernels; it
+  // forks from and joins back into `stream` within one library call
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   std::string err;
   uint64_t launches = 0;
   phys_timings tm{};
@@ -188,13 +192,16 @@ int diagnostics(phys_ctx* c, double G, double* out5);
 int probe_peaks(phys_ctx* c, double* fp32, double* fp32x2, double* fp64);
 }  // namespace phys
 
-#define PHYS_LAUNCH(c, kernel, grid, block, smem, ...)                     \
+#define PHYS_LAUNCH_ON(c, strm, kernel, grid, block, smem, ...)            \
   do {                                                                     \
-    kernel<<<(grid), (block), (smem), (c)->stream>>>(__VA_ARGS__);          \
+    kernel<<<(grid), (block), (smem), (strm)>>>(__VA_ARGS__);              \
     (c)->launches++;                                                       \
     int _st = phys::check_launch((c), #kernel);                            \
     if (_st) return _st;                                                   \
   } while (0)
+
+#define PHYS_LAUNCH(c, kernel, grid, block, smem, ...) \
+  PHYS_LAUNCH_ON(c, (c)->stream, kernel, grid, block, smem, __VA_ARGS__)
 
 #define PHYS_CUDA(c, call)                                                 \
   do {                                                                     \

@@ -344,6 +344,15 @@ int phys_ctx_create(int device, phys_ctx** out) {
     for (auto& ev : c->ev)
       if ((e = cudaEventCreate(&ev)) != cudaSuccess) { st = cuda_fail(c, e, "cudaEventCreate"); break; }
     if (st) break;
+    if ((e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking)) != cudaSuccess) {
+      st = cuda_fail(c, e, "cudaStreamCreate(side)");
+      break;
+    }
+    if ((e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming)) != cudaSuccess) {
+      st = cuda_fail(c, e, "cudaEventCreate(fork/join)");
+      break;
+    }
     char* small = nullptr;
     if ((e = cudaMalloc(&small, 4096)) != cudaSuccess) { st = cuda_fail(c, e, "cudaMalloc(small)"); break; }
     c->d_status = reinterpret_cast<int32_t*>(small);
@@ -369,6 +378,7 @@ int phys_ctx_create(int device, phys_ctx** out) {
 int phys_ctx_destroy(phys_ctx* c) {
   if (!c) return PHYS_OK;
   cudaSetDevice(c->device);
+  if (c->side) cudaStreamSynchronize(c->side);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (auto& b : c->ws)
     if (b.p) cudaFree(b.p);
@@ -380,6 +390,9 @@ int phys_ctx_destroy(phys_ctx* c) {
   if (c->h_small) cudaFreeHost(c->h_small);
   for (auto& ev : c->ev)
     if (ev) cudaEventDestroy(ev);
+  if (c->fork) cudaEventDestroy(c->fork);
+  if (c->join) cudaEventDestroy(c->join);
+  if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   cudaGetLastError();
   delete c;

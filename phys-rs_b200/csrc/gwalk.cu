@@ -28,7 +28,9 @@
 //      through shared memory (cp.async, two batches in flight), then every
 //      lane accumulates its two targets over the batch (broadcast loads);
 //   3. gwalk_kernel walks and evaluates the re-queued subgroups in one pass
-//      (list in shared memory, evaluated whenever it fills).
+//      (list in shared memory, evaluated whenever it fills), on a second
+//      stream beside geval_kernel: these are a few hundred serial walks at
+//      most, bound by the latency of their tree reads, not by throughput.
 // The list arithmetic is the per-body walk's: F64 = f64 FMA + rsqrt on
 // absolute coordinates; F32C = f32 pair terms on double-float coordinates
 // relative to the group's first body, r = (hi_j - hi_i) + (lo_j - lo_i), two
@@ -59,7 +61,7 @@
 #define GWALK_LIST_LIMIT 8192
 #endif
 #ifndef GWALK_SPLIT
-#define GWALK_SPLIT 4
+#define GWALK_SPLIT 1
 #endif
 #ifndef GWALK_FAR
 #define GWALK_FAR 0.5
@@ -1000,14 +1002,23 @@ int launch(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force, 
   PHYS_LAUNCH(c, glist_kernel, grid_list, kLBlock, kLSmem, (int)n, (int)t.nnodes, t.gnode,
               t.groups, t.ngroups, ctr, t.body64, theta2f, pool, pool_per_warp, items, ctr + 2,
               retry, ctr + 1, c->d_status);
+  // The re-queued subgroups (a few hundred serial, latency-bound walks at
+  // most) run on the side stream beside the list evaluation; it is launched
+  // first so that its warps holding work are resident from the start.  Both
+  // kernels write disjoint bodies and add to the counters atomically; the
+  // main stream joins the side stream before anything reads the results.
+  PHYS_CUDA(c, cudaEventRecord(c->fork, c->stream));
+  PHYS_CUDA(c, cudaStreamWaitEvent(c->side, c->fork, 0));
+  PHYS_LAUNCH_ON(c, c->side, gwalk_kernel<kF32>, grid_fused, kGBlock, kGSmem, (int)n,
+                 (int)t.nnodes, t.gnode, retry, ctr + 1, ctr + 4, t.body64, t.perm, p->G, eps2,
+                 theta2f, (int)want_force, ox, oy, oz, c->d_counter, c->d_status);
+  PHYS_CUDA(c, cudaEventRecord(c->join, c->side));
   PHYS_CUDA(c, cudaEventRecord(c->ev[10], c->stream));
   PHYS_LAUNCH(c, geval_kernel<kF32>, grid_eval, kGBlock, kESmem, (int)n, t.gnode, items, ctr + 2,
               ctr + 3, pool, t.body64, t.perm, p->G, eps2, (int)want_force, ox, oy, oz,
               c->d_counter, c->d_status);  // adds to counter[0] and counter[1]
   PHYS_CUDA(c, cudaEventRecord(c->ev[11], c->stream));
-  PHYS_LAUNCH(c, gwalk_kernel<kF32>, grid_fused, kGBlock, kGSmem, (int)n, (int)t.nnodes, t.gnode,
-              retry, ctr + 1, ctr + 4, t.body64, t.perm, p->G, eps2, theta2f, (int)want_force, ox,
-              oy, oz, c->d_counter, c->d_status);
+  PHYS_CUDA(c, cudaStreamWaitEvent(c->stream, c->join, 0));
   return PHYS_OK;
 }
 
