@@ -438,6 +438,55 @@ struct Evaluator {
     sz = fma(rz, w, sz);
   }
 
+  // Near chunks [q0, q1) of the list (double-float offsets) against the
+  // lane's target a, and target b when kTwo.  One instantiation per target
+  // count keeps all of a chunk's terms in one basic block, free to
+  // interleave.
+  template <bool kSelf, bool kTwo>
+  __device__ __forceinline__ void near_chunks(int q0, int q1) {
+    const float4* HX = reinterpret_cast<const float4*>(f);
+    const float4* HY = reinterpret_cast<const float4*>(f + kL);
+    const float4* HZ = reinterpret_cast<const float4*>(f + 2 * kL);
+    const float4* MM = reinterpret_cast<const float4*>(f + 3 * kL);
+    const float4* LX = reinterpret_cast<const float4*>(f + 4 * kL);
+    const float4* LY = reinterpret_cast<const float4*>(f + 5 * kL);
+    const float4* LZ = reinterpret_cast<const float4*>(f + 6 * kL);
+#pragma unroll kEvalUnroll
+    for (int q = q0; q < q1; ++q) {
+      const float4 hx = HX[q], hy = HY[q], hz = HZ[q], mm = MM[q];
+      const float4 lx = LX[q], ly = LY[q], lz = LZ[q];
+      // in-group pass, the target's own slot: two per lane: target a is
+      // slot 2*lane, target b 2*lane + 1 (chunk lane/2, pair lane & 1);
+      // one per lane: slot lane (chunk lane/4, pair (lane/2) & 1, half
+      // lane & 1)
+      bool a0e = false, a0f = false, a1e = false, a1f = false, b0 = false, b1 = false;
+      if (kSelf) {
+        if (kTwo) {
+          const bool in = q == (lane >> 1);
+          a0e = b0 = in && !(lane & 1);
+          a1e = b1 = in && (lane & 1);
+        } else {
+          const bool in = q == (lane >> 2);
+          const bool p1 = (lane >> 1) & 1, h1 = lane & 1;
+          a0e = in && !p1 && !h1;
+          a0f = in && !p1 && h1;
+          a1e = in && p1 && !h1;
+          a1f = in && p1 && h1;
+        }
+      }
+      term32(lo2(hx), lo2(hy), lo2(hz), lo2(mm), lo2(lx), lo2(ly), lo2(lz), nhxa, nhya, nhza,
+             nlxa, nlya, nlza, a0e, a0f, pxa, pya, pza);
+      term32(hi2(hx), hi2(hy), hi2(hz), hi2(mm), hi2(lx), hi2(ly), hi2(lz), nhxa, nhya, nhza,
+             nlxa, nlya, nlza, a1e, a1f, pxa, pya, pza);
+      if (kTwo) {
+        term32(lo2(hx), lo2(hy), lo2(hz), lo2(mm), lo2(lx), lo2(ly), lo2(lz), nhxb, nhyb, nhzb,
+               nlxb, nlyb, nlzb, false, b0, pxb, pyb, pzb);
+        term32(hi2(hx), hi2(hy), hi2(hz), hi2(mm), hi2(lx), hi2(ly), hi2(lz), nhxb, nhyb, nhzb,
+               nlxb, nlyb, nlzb, false, b1, pxb, pyb, pzb);
+      }
+    }
+  }
+
   // Evaluates list slots [0, nl) for both targets (warp-collective).
   template <bool kSelf>
   __device__ __forceinline__ void eval(int nl) {
@@ -451,49 +500,12 @@ struct Evaluator {
       }
       __syncwarp();
       const int nq = np >> 2;
-      const float4* HX = reinterpret_cast<const float4*>(f);
-      const float4* HY = reinterpret_cast<const float4*>(f + kL);
-      const float4* HZ = reinterpret_cast<const float4*>(f + 2 * kL);
-      const float4* MM = reinterpret_cast<const float4*>(f + 3 * kL);
-      const float4* LX = reinterpret_cast<const float4*>(f + 4 * kL);
-      const float4* LY = reinterpret_cast<const float4*>(f + 5 * kL);
-      const float4* LZ = reinterpret_cast<const float4*>(f + 6 * kL);
       for (int q0 = 0; q0 < nq;) {
         const int q1 = min(q0 + (kFlushChunks - pend), nq);
-#pragma unroll kEvalUnroll
-        for (int q = q0; q < q1; ++q) {
-          const float4 hx = HX[q], hy = HY[q], hz = HZ[q], mm = MM[q];
-          const float4 lx = LX[q], ly = LY[q], lz = LZ[q];
-          // in-group pass, the target's own slot: two per lane: target a is
-          // slot 2*lane, target b 2*lane + 1 (chunk lane/2, pair lane & 1);
-          // one per lane: slot lane (chunk lane/4, pair (lane/2) & 1, half
-          // lane & 1)
-          bool a0e = false, a0f = false, a1e = false, a1f = false, b0 = false, b1 = false;
-          if (kSelf) {
-            if (two) {
-              const bool in = q == (lane >> 1);
-              a0e = b0 = in && !(lane & 1);
-              a1e = b1 = in && (lane & 1);
-            } else {
-              const bool in = q == (lane >> 2);
-              const bool p1 = (lane >> 1) & 1, h1 = lane & 1;
-              a0e = in && !p1 && !h1;
-              a0f = in && !p1 && h1;
-              a1e = in && p1 && !h1;
-              a1f = in && p1 && h1;
-            }
-          }
-          term32(lo2(hx), lo2(hy), lo2(hz), lo2(mm), lo2(lx), lo2(ly), lo2(lz), nhxa, nhya, nhza,
-                 nlxa, nlya, nlza, a0e, a0f, pxa, pya, pza);
-          term32(hi2(hx), hi2(hy), hi2(hz), hi2(mm), hi2(lx), hi2(ly), hi2(lz), nhxa, nhya, nhza,
-                 nlxa, nlya, nlza, a1e, a1f, pxa, pya, pza);
-          if (two) {
-            term32(lo2(hx), lo2(hy), lo2(hz), lo2(mm), lo2(lx), lo2(ly), lo2(lz), nhxb, nhyb,
-                   nhzb, nlxb, nlyb, nlzb, false, b0, pxb, pyb, pzb);
-            term32(hi2(hx), hi2(hy), hi2(hz), hi2(mm), hi2(lx), hi2(ly), hi2(lz), nhxb, nhyb,
-                   nhzb, nlxb, nlyb, nlzb, false, b1, pxb, pyb, pzb);
-          }
-        }
+        if (two)
+          near_chunks<kSelf, true>(q0, q1);
+        else
+          near_chunks<kSelf, false>(q0, q1);
         chunks_done(q1 - q0);
         q0 = q1;
       }
@@ -524,6 +536,25 @@ struct Evaluator {
     pz = __ffma2_rn(rz, w, pz);
   }
 
+  // Far chunks [q0, q1) against target a, and target b when kTwo.
+  template <bool kTwo>
+  __device__ __forceinline__ void far_chunks(int q0, int q1) {
+    const float4* HX = reinterpret_cast<const float4*>(ff);
+    const float4* HY = reinterpret_cast<const float4*>(ff + kL);
+    const float4* HZ = reinterpret_cast<const float4*>(ff + 2 * kL);
+    const float4* MM = reinterpret_cast<const float4*>(ff + 3 * kL);
+#pragma unroll kEvalUnroll
+    for (int q = q0; q < q1; ++q) {
+      const float4 hx = HX[q], hy = HY[q], hz = HZ[q], mm = MM[q];
+      term32f(lo2(hx), lo2(hy), lo2(hz), lo2(mm), nhxa, nhya, nhza, pxa, pya, pza);
+      term32f(hi2(hx), hi2(hy), hi2(hz), hi2(mm), nhxa, nhya, nhza, pxa, pya, pza);
+      if (kTwo) {
+        term32f(lo2(hx), lo2(hy), lo2(hz), lo2(mm), nhxb, nhyb, nhzb, pxb, pyb, pzb);
+        term32f(hi2(hx), hi2(hy), hi2(hz), hi2(mm), nhxb, nhyb, nhzb, pxb, pyb, pzb);
+      }
+    }
+  }
+
   // Evaluates far-list slots [0, nl) for both targets (warp-collective).
   __device__ __forceinline__ void eval_far(int nl) {
     const int np = (nl + 3) & ~3;
@@ -534,22 +565,12 @@ struct Evaluator {
     }
     __syncwarp();
     const int nq = np >> 2;
-    const float4* HX = reinterpret_cast<const float4*>(ff);
-    const float4* HY = reinterpret_cast<const float4*>(ff + kL);
-    const float4* HZ = reinterpret_cast<const float4*>(ff + 2 * kL);
-    const float4* MM = reinterpret_cast<const float4*>(ff + 3 * kL);
     for (int q0 = 0; q0 < nq;) {
       const int q1 = min(q0 + (kFlushChunks - pend), nq);
-#pragma unroll kEvalUnroll
-      for (int q = q0; q < q1; ++q) {
-        const float4 hx = HX[q], hy = HY[q], hz = HZ[q], mm = MM[q];
-        term32f(lo2(hx), lo2(hy), lo2(hz), lo2(mm), nhxa, nhya, nhza, pxa, pya, pza);
-        term32f(hi2(hx), hi2(hy), hi2(hz), hi2(mm), nhxa, nhya, nhza, pxa, pya, pza);
-        if (two) {
-          term32f(lo2(hx), lo2(hy), lo2(hz), lo2(mm), nhxb, nhyb, nhzb, pxb, pyb, pzb);
-          term32f(hi2(hx), hi2(hy), hi2(hz), hi2(mm), nhxb, nhyb, nhzb, pxb, pyb, pzb);
-        }
-      }
+      if (two)
+        far_chunks<true>(q0, q1);
+      else
+        far_chunks<false>(q0, q1);
       chunks_done(q1 - q0);
       q0 = q1;
     }
