@@ -135,6 +135,18 @@ def test_sort_fixup_long_runs(ctx):
     structure_check(ctx, pos, m)
 
 
+@pytest.mark.parametrize("n", [1 << 20, 300_001])
+def test_sort_many_tiles(ctx, n):
+    """The key sort over hundreds of 2048-key tiles (every pass is one kernel
+    whose tiles take their offsets from the tiles before them): the
+    permutation is the stable order of the (hi, lo) descent keys."""
+    pos, _, m = ics.plummer(n, seed=11)
+    ctx.upload(pos, None, m)
+    g = ctx.bh_export(bh(precision=F64))
+    hi, lo = g["keys_hi"], g["keys_lo"]
+    assert np.array_equal(g["perm"], np.lexsort((np.arange(n), lo, hi)))
+
+
 @pytest.mark.parametrize("n,theta,seed", [(1000, 0.5, 1), (4096, 0.5, 2), (4096, 0.0, 3),
                                           (4096, 1.0, 4), (30000, 0.5, 5)])
 def test_exact_forces_bitexact(ctx, n, theta, seed):
