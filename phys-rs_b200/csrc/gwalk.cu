@@ -641,10 +641,10 @@ struct Evaluator {
           const int e = lane + 32 * j;
           const bool valid = e < n_b;
           const double4 src = valid ? buf[e] : X0;
-          float hx, lx, hy, ly, hz, lz;
-          split_df(src.x - X0.x, hx, lx);
-          split_df(src.y - X0.y, hy, ly);
-          split_df(src.z - X0.z, hz, lz);
+          // offsets from X0; their low parts (as split_df) only for near entries
+          const double ox = src.x - X0.x, oy = src.y - X0.y, oz = src.z - X0.z;
+          const float hx = __double2float_rn(ox), hy = __double2float_rn(oy),
+                      hz = __double2float_rn(oz);
           const float dx = fmaxf(fabsf(hx - B.cx) - B.bx, 0.f);
           const float dy = fmaxf(fabsf(hy - B.cy) - B.by, 0.f);
           const float dz = fmaxf(fabsf(hz - B.cz) - B.bz, 0.f);
@@ -664,9 +664,9 @@ struct Evaluator {
             f[kL + q] = hy;
             f[2 * kL + q] = hz;
             f[3 * kL + q] = m;
-            f[4 * kL + q] = lx;
-            f[5 * kL + q] = ly;
-            f[6 * kL + q] = lz;
+            f[4 * kL + q] = __double2float_rn(ox - (double)hx);
+            f[5 * kL + q] = __double2float_rn(oy - (double)hy);
+            f[6 * kL + q] = __double2float_rn(oz - (double)hz);
           }
           nfar += __popc(fm);
           nnear += __popc(nm);
