@@ -14,10 +14,11 @@
  *    "_device".
  *  - Every call returns a status (PHYS_OK == 0).  No call aborts, throws or
  *    traps; on error phys_last_error() describes it.
- *  - A context owns one CUDA stream and all device memory it uses.  It is not
- *    thread-safe (use one context per thread).  Calls are synchronous at
- *    return, like the reference's blocking readback (src/gpu/buffers.rs:163-213),
- *    except phys_verlet_steps_async.
+ *  - A context owns its CUDA streams (a main stream, and a second one that
+ *    forks from and joins back into it within a call) and all device memory
+ *    it uses.  It is not thread-safe (use one context per thread).  Calls
+ *    are synchronous at return, like the reference's blocking readback
+ *    (src/gpu/buffers.rs:163-213), except phys_verlet_steps_async.
  *  - Body state stays resident on the device between calls, so multi-step
  *    runs do not cross PCIe.
  */
@@ -107,7 +108,8 @@ const char* phys_last_error(const phys_ctx* ctx);
 int phys_ctx_create(int device, phys_ctx** out);
 int phys_ctx_destroy(phys_ctx* ctx);
 /* The cudaStream_t the context launches on (for callers that time or order
- * work around it). */
+ * work around it).  Work the context puts on its second stream is joined
+ * back into this one before the call returns or queues anything after it. */
 void* phys_ctx_stream(phys_ctx* ctx);
 int phys_last_timings(const phys_ctx* ctx, phys_timings* out);
 
