@@ -416,6 +416,15 @@ __global__ void compact_kernel(int64_t nnodes, const int4* __restrict__ link,
 // (fixed order: deterministic), propagated bottom-up by the last-arriving
 // child.  Differs from the reference's insertion-order running mean by ulps.
 // ---------------------------------------------------------------------------
+// arrive[] += 1 with acquire-release order at GPU scope; returns the old
+// count.  Orders the caller's earlier stores before it and later loads after
+// it, in place of a fence on each side of a relaxed atomic.
+__device__ __forceinline__ int32_t arrive_acq_rel(int32_t* p) {
+  int32_t old;
+  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(p) : "memory");
+  return old;
+}
+
 __global__ void __launch_bounds__(kBlock)
 com_upward_kernel(int64_t nnodes, const int4* __restrict__ link,
                   const int32_t* __restrict__ parent, const int32_t* __restrict__ nchild,
@@ -436,14 +445,14 @@ com_upward_kernel(int64_t nnodes, const int4* __restrict__ link,
     sums[k] = make_double4(sx, sy, sz, sm);
     int32_t cur = (int32_t)k;
     while (cur != 0) {
-      __threadfence();
       const int32_t par = parent[cur];
       if (par < 0 || par >= cur) {  // parents precede children in pre-order
         atomicOr(status, kStatOverflow);
         break;
       }
-      if (atomicAdd(&arrive[par], 1) != nchild[par] - 1) break;
-      __threadfence();
+      // release: this child's sums are visible to whoever arrives last;
+      // acquire: the last arrival sees every sibling's sums
+      if (arrive_acq_rel(&arrive[par]) != nchild[par] - 1) break;
       const int32_t stop = link[par].x;
       double ax = 0.0, ay = 0.0, az = 0.0, am = 0.0;
       int guard = 0;
