@@ -64,7 +64,7 @@
 #define GWALK_SPLIT 1
 #endif
 #ifndef GWALK_FAR
-#define GWALK_FAR 0.5
+#define GWALK_FAR 0.25
 #endif
 #ifndef GEVAL_UNROLL
 #define GEVAL_UNROLL 2
@@ -586,8 +586,8 @@ struct Evaluator {
   // distance from the group's box is at least GWALK_FAR box half-diagonals b
   // goes to the far list, whose plain f32 offsets from X0 need no low parts
   // (targets lie within 2b of X0, so the separation's error is below
-  // 2^-24 (2|r| + 4b) <= 10 * 2^-24 |r| at 0.5 half-diagonals, the size of
-  // the f32 pair term's own rounding); the rest go to the near list
+  // 2^-24 (2|r| + 4b) <= 18 * 2^-24 |r| at a quarter half-diagonal, a few
+  // times the f32 pair term's own rounding); the rest go to the near list
   // (double-float).  F64: the staged
   // records are the list.
   __device__ __forceinline__ void stream_eval(const uint32_t* __restrict__ codes, int len,
