@@ -116,6 +116,10 @@ static_assert((kGRecOff + 5 * 32 * 4) % 16 == 0, "record alignment");
 
 __device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
 __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
+// Two consecutive floats from an 8-byte-aligned shared-memory address.
+__device__ __forceinline__ float2 ld2(const float* p) {
+  return *reinterpret_cast<const float2*>(p);
+}
 
 __device__ __forceinline__ double4 ldg_d4(const double4* p) {
   const double2* q = reinterpret_cast<const double2*>(p);
@@ -314,11 +318,18 @@ __device__ __forceinline__ int traverse(int lane, int base, int gend, int nnodes
 // The F32C list in shared memory is a structure of arrays (slot-consecutive
 // writes hit distinct banks; the evaluation reads four entries per 16-byte
 // load).
+// Target layouts: one per lane (at most 32 bodies); two per lane, 2l and
+// 2l + 1 (33..64 bodies; F32C 49..64); F32C 33..48 bodies: target a = l and
+// target b = 32 + l mod (32 / rb), the lanes of b split into rb = 2 (41..48
+// bodies) or 4 (33..40) streams that each take a 1/rb share of the list's
+// entries for b, so that the second slot carries no idle lanes; the
+// streams' sums for b are added at the end.
 template <bool kF32, int kL>
 struct Evaluator {
   int lane, nvalid, ia, ib;
   bool va, vb;
-  bool two;  // two targets per lane (more than 32 bodies), else one
+  bool two;  // a second target per lane (more than 32 bodies), else one
+  int rb;    // streams sharing each b target (2 or 4), 0: one lane per target
   double4 X0, ta, tb;
   double eps2;
   float* f;        // F32C list: hx, hy, hz, m, lx, ly, lz arrays of kL
@@ -337,8 +348,14 @@ struct Evaluator {
     lane = lane_;
     nvalid = gend - base;
     two = nvalid > 32;
-    ia = two ? base + 2 * lane : base + lane;
-    ib = two ? ia + 1 : gend;
+    rb = (kF32 && two && nvalid <= 48) ? (nvalid <= 40 ? 4 : 2) : 0;
+    if (rb) {
+      ia = base + lane;
+      ib = base + 32 + lane % (32 / rb);
+    } else {
+      ia = two ? base + 2 * lane : base + lane;
+      ib = two ? ia + 1 : gend;
+    }
     va = ia < gend;
     vb = ib < gend;
     X0 = body64[base];
@@ -487,12 +504,62 @@ struct Evaluator {
     }
   }
 
+  // Near chunks [q0, q1) (q1 - q0 even) in the split layout: target a takes
+  // both chunks of a pair, target b the share of this lane's stream (kR = 2:
+  // one chunk, kR = 4: one entry pair), read with its own loads.
+  template <bool kSelf, int kR>
+  __device__ __forceinline__ void near_split(int q0, int q1) {
+    const float4* HX = reinterpret_cast<const float4*>(f);
+    const float4* HY = reinterpret_cast<const float4*>(f + kL);
+    const float4* HZ = reinterpret_cast<const float4*>(f + 2 * kL);
+    const float4* MM = reinterpret_cast<const float4*>(f + 3 * kL);
+    const float4* LX = reinterpret_cast<const float4*>(f + 4 * kL);
+    const float4* LY = reinterpret_cast<const float4*>(f + 5 * kL);
+    const float4* LZ = reinterpret_cast<const float4*>(f + 6 * kL);
+    constexpr int kLps = 32 / kR;                      // lanes per stream
+    const int st = lane / kLps, tb = 32 + lane % kLps;  // stream, b's slot
+    const int pa = lane & 3;                            // a's slot: chunk lane/4
+    for (int q = q0; q < q1; q += 2) {
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const int qa = q + k;
+        const float4 hx = HX[qa], hy = HY[qa], hz = HZ[qa], mm = MM[qa];
+        const float4 lx = LX[qa], ly = LY[qa], lz = LZ[qa];
+        const bool in = kSelf && qa == (lane >> 2);
+        term32(lo2(hx), lo2(hy), lo2(hz), lo2(mm), lo2(lx), lo2(ly), lo2(lz), nhxa, nhya, nhza,
+               nlxa, nlya, nlza, in && pa == 0, in && pa == 1, pxa, pya, pza);
+        term32(hi2(hx), hi2(hy), hi2(hz), hi2(mm), hi2(lx), hi2(ly), hi2(lz), nhxa, nhya, nhza,
+               nlxa, nlya, nlza, in && pa == 2, in && pa == 3, pxa, pya, pza);
+      }
+      if (kR == 2) {
+        const int qb = q + st;
+        const float4 hx = HX[qb], hy = HY[qb], hz = HZ[qb], mm = MM[qb];
+        const float4 lx = LX[qb], ly = LY[qb], lz = LZ[qb];
+        const bool in = kSelf && qb == (tb >> 2);
+        const int pb = tb & 3;
+        term32(lo2(hx), lo2(hy), lo2(hz), lo2(mm), lo2(lx), lo2(ly), lo2(lz), nhxb, nhyb, nhzb,
+               nlxb, nlyb, nlzb, in && pb == 0, in && pb == 1, pxb, pyb, pzb);
+        term32(hi2(hx), hi2(hy), hi2(hz), hi2(mm), hi2(lx), hi2(ly), hi2(lz), nhxb, nhyb, nhzb,
+               nlxb, nlyb, nlzb, in && pb == 2, in && pb == 3, pxb, pyb, pzb);
+      } else {
+        const int e = 4 * q + 2 * st;  // the stream's entry pair (e, e + 1)
+        const float2 hx = ld2(f + e), hy = ld2(f + kL + e), hz = ld2(f + 2 * kL + e);
+        const float2 mm = ld2(f + 3 * kL + e);
+        const float2 lx = ld2(f + 4 * kL + e), ly = ld2(f + 5 * kL + e),
+                     lz = ld2(f + 6 * kL + e);
+        term32(hx, hy, hz, mm, lx, ly, lz, nhxb, nhyb, nhzb, nlxb, nlyb, nlzb,
+               kSelf && e == tb, kSelf && e + 1 == tb, pxb, pyb, pzb);
+      }
+    }
+  }
+
   // Evaluates list slots [0, nl) for both targets (warp-collective).
   template <bool kSelf>
   __device__ __forceinline__ void eval(int nl) {
     if (kF32) {
-      // pad to a multiple of 4 with massless entries far away
-      const int np = (nl + 3) & ~3;
+      // pad to a multiple of 4 (split layout: 8) with massless entries far
+      // away
+      const int np = rb ? (nl + 7) & ~7 : (nl + 3) & ~3;
       if (lane < np - nl) {
         const int s = nl + lane;
         f[s] = f[kL + s] = f[2 * kL + s] = 1e15f;
@@ -502,7 +569,11 @@ struct Evaluator {
       const int nq = np >> 2;
       for (int q0 = 0; q0 < nq;) {
         const int q1 = min(q0 + (kFlushChunks - pend), nq);
-        if (two)
+        if (rb == 4)
+          near_split<kSelf, 4>(q0, q1);
+        else if (rb == 2)
+          near_split<kSelf, 2>(q0, q1);
+        else if (two)
           near_chunks<kSelf, true>(q0, q1);
         else
           near_chunks<kSelf, false>(q0, q1);
@@ -555,9 +626,38 @@ struct Evaluator {
     }
   }
 
+  // Far chunks [q0, q1) (q1 - q0 even) in the split layout (as near_split).
+  template <int kR>
+  __device__ __forceinline__ void far_split(int q0, int q1) {
+    const float4* HX = reinterpret_cast<const float4*>(ff);
+    const float4* HY = reinterpret_cast<const float4*>(ff + kL);
+    const float4* HZ = reinterpret_cast<const float4*>(ff + 2 * kL);
+    const float4* MM = reinterpret_cast<const float4*>(ff + 3 * kL);
+    constexpr int kLps = 32 / kR;
+    const int st = lane / kLps;
+    for (int q = q0; q < q1; q += 2) {
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const float4 hx = HX[q + k], hy = HY[q + k], hz = HZ[q + k], mm = MM[q + k];
+        term32f(lo2(hx), lo2(hy), lo2(hz), lo2(mm), nhxa, nhya, nhza, pxa, pya, pza);
+        term32f(hi2(hx), hi2(hy), hi2(hz), hi2(mm), nhxa, nhya, nhza, pxa, pya, pza);
+      }
+      if (kR == 2) {
+        const int qb = q + st;
+        const float4 hx = HX[qb], hy = HY[qb], hz = HZ[qb], mm = MM[qb];
+        term32f(lo2(hx), lo2(hy), lo2(hz), lo2(mm), nhxb, nhyb, nhzb, pxb, pyb, pzb);
+        term32f(hi2(hx), hi2(hy), hi2(hz), hi2(mm), nhxb, nhyb, nhzb, pxb, pyb, pzb);
+      } else {
+        const int e = 4 * q + 2 * st;
+        term32f(ld2(ff + e), ld2(ff + kL + e), ld2(ff + 2 * kL + e), ld2(ff + 3 * kL + e), nhxb,
+                nhyb, nhzb, pxb, pyb, pzb);
+      }
+    }
+  }
+
   // Evaluates far-list slots [0, nl) for both targets (warp-collective).
   __device__ __forceinline__ void eval_far(int nl) {
-    const int np = (nl + 3) & ~3;
+    const int np = rb ? (nl + 7) & ~7 : (nl + 3) & ~3;
     if (lane < np - nl) {
       const int s = nl + lane;
       ff[s] = ff[kL + s] = ff[2 * kL + s] = 1e15f;
@@ -567,7 +667,11 @@ struct Evaluator {
     const int nq = np >> 2;
     for (int q0 = 0; q0 < nq;) {
       const int q1 = min(q0 + (kFlushChunks - pend), nq);
-      if (two)
+      if (rb == 4)
+        far_split<4>(q0, q1);
+      else if (rb == 2)
+        far_split<2>(q0, q1);
+      else if (two)
         far_chunks<true>(q0, q1);
       else
         far_chunks<false>(q0, q1);
@@ -694,8 +798,13 @@ struct Evaluator {
 
   // Pairs inside the group, exact, i != j.
   __device__ __forceinline__ void self_pass() {
-    if (va) put(two ? 2 * lane : lane, ta);
-    if (vb) put(2 * lane + 1, tb);
+    if (rb) {
+      if (va) put(lane, ta);
+      if (vb && lane < 32 / rb) put(32 + lane, tb);
+    } else {
+      if (va) put(two ? 2 * lane : lane, ta);
+      if (vb) put(2 * lane + 1, tb);
+    }
     eval<true>(nvalid);
   }
 
@@ -719,8 +828,16 @@ struct Evaluator {
       flush();  // the partials of the last chunks
       if (va) out(ia, (double)Hx.x + (double)Lx.x, (double)Hy.x + (double)Ly.x,
                   (double)Hz.x + (double)Lz.x);
-      if (vb) out(ib, (double)Hx.y + (double)Lx.y, (double)Hy.y + (double)Ly.y,
-                  (double)Hz.y + (double)Lz.y);
+      double bx_ = (double)Hx.y + (double)Lx.y, by_ = (double)Hy.y + (double)Ly.y,
+             bz_ = (double)Hz.y + (double)Lz.y;
+      if (rb) {  // add the streams' sums of the same b target
+        for (int o = 32 / rb; o < 32; o <<= 1) {
+          bx_ += __shfl_xor_sync(kFull, bx_, o);
+          by_ += __shfl_xor_sync(kFull, by_, o);
+          bz_ += __shfl_xor_sync(kFull, bz_, o);
+        }
+      }
+      if (vb && (!rb || lane < 32 / rb)) out(ib, bx_, by_, bz_);
     } else {
       if (va) out(ia, ax, ay, az);
       if (vb) out(ib, bx, by, bz);
