@@ -26,7 +26,8 @@
 //      subgroups of kGSplit consecutive bodies, whose lists are far shorter;
 //   2. geval_kernel evaluates the lists: batches of kEB entries stream
 //      through shared memory (cp.async, two batches in flight), then every
-//      lane accumulates its two targets over the batch (broadcast loads);
+//      lane accumulates its one or two targets over the batch (broadcast
+//      loads; the target layouts are described at Evaluator);
 //   3. gwalk_kernel walks and evaluates the re-queued subgroups in one pass
 //      (list in shared memory, evaluated whenever it fills), on a second
 //      stream beside geval_kernel: these are a few hundred serial walks at
