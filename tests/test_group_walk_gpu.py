@@ -39,6 +39,21 @@ def test_theta_zero_is_direct_sum(ctx, n, leaf_cap):
     assert ctx.timings()["interactions"] == n * (n - 1)
 
 
+@pytest.mark.parametrize("n", [8, 9, 16, 17, 32, 33, 40, 41, 48, 49])
+def test_single_group_layouts_theta_zero(ctx, n):
+    """Systems of at most 64 bodies are one group: at theta = 0 every body
+    of every target layout (one per lane; a second target shared by 4 lane
+    streams at 33-40 bodies or 2 at 41-48; two per lane above) must match the
+    direct sum, the in-group pass skipping exactly i == j."""
+    pos, _, m = ics.plummer(n, seed=100 + n)
+    ctx.upload(pos, None, m)
+    ref = oracle.direct_forces(pos, m, 1.0, 0.01)
+    f32 = ctx.gravity_forces(gw(0.0, F32C, 8))
+    assert ctx.timings()["interactions"] == n * (n - 1)
+    e = rel_err(f32, ref)
+    assert np.median(e) < 1e-6 and e.max() < 1e-4
+
+
 @pytest.mark.parametrize("leaf_cap", [1, 8, 16])
 def test_f32c_vs_f64_same_lists(ctx, leaf_cap):
     pos, _, m = ics.plummer(65536, seed=21)
