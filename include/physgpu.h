@@ -5,8 +5,8 @@
  * The reference has no FFI for this path: its "plugin API" is a set of
  * bevy_ecs system functions registered in a Schedule (src/main.rs:103-140).
  * Each entry point below names the reference system or code whose work it
- * replaces, so a Rust `extern "C"` block can wrap them
- * in systems of the same signatures.
+ * replaces, so a Rust `extern "C"` block can wrap them in systems of the
+ * same signatures.
  *
  * Conventions
  *  - Plain pointers and sizes; arrays are structure-of-arrays, f64, length n,
@@ -16,7 +16,9 @@
  *    traps; on error phys_last_error() describes it.
  *  - A context owns its CUDA streams (a main stream, and a second one that
  *    forks from and joins back into it within a call) and all device memory
- *    it uses.  It is not thread-safe (use one context per thread).  Calls
+ *    it uses.  It is not thread-safe (use one context per thread); contexts
+ *    share no state, and every call makes its context's device current, so
+ *    contexts on several devices may be used from one thread.  Calls
  *    are synchronous at return, like the reference's blocking readback
  *    (src/gpu/buffers.rs:163-213), except phys_verlet_steps_async.
  *  - Body state stays resident on the device between calls, so multi-step
@@ -317,13 +319,27 @@ int phys_bh_export(phys_ctx* ctx, const phys_params* p, int64_t cap, int64_t* nn
  * fixed device array of about 7.3 MiB that every GPU loading the library
  * keeps until the process exits.  The first call on each device looks up the
  * array's device address (cudaGetSymbolAddress) and should come before any
- * stream capture.  All calls share the array, so calls that overlap on the
- * GPU race: order them.  n outside 0..32768 returns PHYS_ERR_ARG with a
+ * stream capture; the address is kept for the life of the process, so a
+ * process that calls cudaDeviceReset on a device must not call this entry
+ * point on that device again.  All calls share the array, so calls that
+ * overlap on the GPU race: order them.  n outside 0..32768 returns PHYS_ERR_ARG with a
  * message in errbuf (optional, errlen bytes).  Synchronous at return. */
 int phys_direct_accel_noalloc(int64_t n, const double* x, const double* y, const double* z,
                               const double* m, double G, double eps, int32_t precision,
                               double* ax, double* ay, double* az, void* stream, char* errbuf,
                               size_t errlen);
+
+/* ---- failure injection for tests ---------------------------------------- */
+/* No counterpart in the reference.  Sets the bound on each bounded device
+ * wait of this context's radix sorts (re-reads of a predecessor tile's status
+ * word; default 2^20, restored by spins < 0).  With a bound of 0 the first
+ * wait gives up at once, as a stalled predecessor would after the default
+ * bound: the evaluation then stops before building on the unfinished order
+ * and returns PHYS_ERR_TIMEOUT, and the context stays usable.  Whether a wait
+ * occurs at all depends on how the sort's tiles are scheduled, so a caller
+ * that wants to see the timeout needs a sort of many tiles (e.g. 2^20
+ * bodies). */
+int phys_debug_set_wait_limit(phys_ctx* ctx, int64_t spins);
 
 /* ---- measured pipe peaks (roofline denominators) ----------------------- */
 /* Times FFMA, packed FFMA2 (f32x2) and DFMA loops on every SM; returns

@@ -82,6 +82,19 @@ struct phys_ctx {
   bool ens_accel_valid = false;
   int ens_group = 0;           // autotuned group size (0: not tuned)
 
+  // ---- per-device launch data, kept per context ----
+  // A kernel's dynamic shared-memory limit (cudaFuncSetAttribute) is set on
+  // the device that is current when it is raised, so it is raised once per
+  // context, after the context has made its own device current; nothing is
+  // shared between contexts or threads.  occ_gwalk: resident blocks per SM of
+  // the group-walk kernels (list, evaluation F64 / F32C, fused walk F64 /
+  // F32C), 0 until queried.
+  int occ_gwalk[5] = {};
+  bool sort_smem_set = false;
+  // Bound on one look-back wait of the radix sort, in re-reads of a tile's
+  // status word (see sort.cu); phys_debug_set_wait_limit lowers it in tests.
+  int64_t sort_spin_limit = int64_t(1) << 20;
+
   // ---- small device scalars ----
   int32_t* d_status = nullptr;               // kStat* bits
   unsigned long long* d_counter = nullptr;   // interaction counter
@@ -148,10 +161,12 @@ int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, 
                 double* oz);
 int direct_targets(phys_ctx* c, const phys_params* p, int64_t nt, const int64_t* d_tidx,
                    double* ox, double* oy, double* oz);
-int direct_accel_launch_scratch(cudaStream_t s, int64_t n, const double* x, const double* y,
-                                const double* z, const double* m, double G, double eps,
-                                int precision, int64_t nslices, double* part, float4* bh,
-                                float4* bl, int32_t* status, double* ox, double* oy, double* oz);
+// Launches on stream s with caller-provided scratch; returns the launch error.
+cudaError_t direct_accel_launch_scratch(cudaStream_t s, int64_t n, const double* x,
+                                        const double* y, const double* z, const double* m,
+                                        double G, double eps, int precision, int64_t nslices,
+                                        double* part, float4* bh, float4* bl, int32_t* status,
+                                        double* ox, double* oy, double* oz);
 // tree.cu
 int bh_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, double* oy,
             double* oz);
@@ -246,6 +261,16 @@ __device__ __forceinline__ float rsqrt_sfu(float x) {
   float y;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
+}
+
+// True when a radix sort earlier in this call gave up a bounded wait
+// (kStatTimeout in the status word): its output need not be a permutation.
+// Kernels that index with a sort's output, or read records built from one,
+// return at once, and the call fails with PHYS_ERR_TIMEOUT.  The flag is
+// written by kernels earlier on the same stream (or on a stream that waited
+// for them), so a later launch reads it settled.
+__device__ __forceinline__ bool sort_failed(const int32_t* status) {
+  return (*reinterpret_cast<const volatile int32_t*>(status) & kStatTimeout) != 0;
 }
 
 // Split a double into a float pair with hi + lo ~= v to ~2^-48 relative.

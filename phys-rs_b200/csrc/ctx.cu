@@ -96,6 +96,15 @@ int read_status(phys_ctx* c, int32_t* out) {
 
 using namespace phys;
 
+// Every entry point that touches the device makes the context's device
+// current first, so contexts on different devices can be used from one
+// thread in any order.
+#define PHYS_ENTER(c)                                    \
+  do {                                                   \
+    if (!(c)) return PHYS_ERR_ARG;                       \
+    PHYS_CUDA((c), cudaSetDevice((c)->device));          \
+  } while (0)
+
 namespace {
 
 int ensure_state(phys_ctx* c, int64_t n) {
@@ -412,10 +421,9 @@ int64_t phys_state_size(const phys_ctx* c) { return c ? c->n : -1; }
 
 int phys_state_upload(phys_ctx* c, int64_t n, const double* x, const double* y, const double* z,
                       const double* vx, const double* vy, const double* vz, const double* m) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (n < 0 || n > (int64_t(1) << 31) - 1) return fail(c, PHYS_ERR_ARG, "n=%lld out of range", (long long)n);
   if (n > 0 && (!x || !y || !z || !m)) return fail(c, PHYS_ERR_ARG, "positions and masses are required");
-  PHYS_CUDA(c, cudaSetDevice(c->device));
   PHYS_TRY(ensure_state(c, n));
   c->n = n;
   c->sector_mode = false;
@@ -443,11 +451,10 @@ int phys_state_upload_sectors(phys_ctx* c, int64_t n, const int64_t* sx, const i
                               const double* lz, double sector_size, int32_t bh_quirk,
                               const double* vx, const double* vy, const double* vz,
                               const double* m) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (n < 0 || n > (int64_t(1) << 31) - 1) return fail(c, PHYS_ERR_ARG, "n out of range");
   if (n > 0 && (!sx || !sy || !sz || !lx || !ly || !lz || !m))
     return fail(c, PHYS_ERR_ARG, "sectors, local positions and masses are required");
-  PHYS_CUDA(c, cudaSetDevice(c->device));
   PHYS_TRY(ensure_state(c, n));
   c->n = n;
   c->sector_mode = false;
@@ -483,12 +490,11 @@ int phys_state_upload_sector_state(phys_ctx* c, int64_t n, const int64_t* sx, co
                                    const int64_t* sz, const double* lx, const double* ly,
                                    const double* lz, double sector_size, const double* vx,
                                    const double* vy, const double* vz, const double* m) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (n < 0 || n > (int64_t(1) << 31) - 1) return fail(c, PHYS_ERR_ARG, "n out of range");
   if (n > 0 && (!sx || !sy || !sz || !lx || !ly || !lz || !m))
     return fail(c, PHYS_ERR_ARG, "sectors, local positions and masses are required");
   if (!(sector_size > 0.0)) return fail(c, PHYS_ERR_ARG, "sector_size must be > 0");
-  PHYS_CUDA(c, cudaSetDevice(c->device));
   PHYS_TRY(ensure_state(c, n));
   PHYS_TRY(sector_state_alloc(c, n));
   c->n = n;
@@ -516,7 +522,7 @@ int phys_state_upload_sector_state(phys_ctx* c, int64_t n, const int64_t* sx, co
 
 int phys_state_download_sector_state(phys_ctx* c, int64_t* sx, int64_t* sy, int64_t* sz,
                                      double* lx, double* ly, double* lz) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (!c->sector_mode) return fail(c, PHYS_ERR_STATE, "no sector state uploaded");
   const int64_t n = c->n, cap = c->sec_cap;
   if (n == 0) return PHYS_OK;
@@ -533,7 +539,7 @@ int phys_state_download_sector_state(phys_ctx* c, int64_t* sx, int64_t* sy, int6
 }
 
 int phys_state_set_accel(phys_ctx* c, const double* ax, const double* ay, const double* az) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (!ax || !ay || !az) return fail(c, PHYS_ERR_ARG, "accelerations are required");
   PHYS_TRY(h2d(c, c->ax, ax, c->n));
   PHYS_TRY(h2d(c, c->ay, ay, c->n));
@@ -546,7 +552,7 @@ int phys_state_set_accel(phys_ctx* c, const double* ax, const double* ay, const 
 
 int phys_state_download(phys_ctx* c, double* x, double* y, double* z, double* vx, double* vy,
                         double* vz, double* ax, double* ay, double* az) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   int64_t n = c->n;
   if (n == 0) return PHYS_OK;
   const int64_t cap = c->sec_cap;
@@ -586,7 +592,7 @@ static int comp_ptrs(phys_ctx* c, int32_t comp, double** a, double** b, double**
 
 int phys_component_write(phys_ctx* c, int32_t comp, const double* a, const double* b,
                          const double* d) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (c->n == 0) return fail(c, PHYS_ERR_STATE, "no body state uploaded");
   double *da = nullptr, *db = nullptr, *dd = nullptr;
   PHYS_TRY(comp_ptrs(c, comp, &da, &db, &dd));
@@ -606,7 +612,7 @@ int phys_component_write(phys_ctx* c, int32_t comp, const double* a, const doubl
 }
 
 int phys_component_read(phys_ctx* c, int32_t comp, double* a, double* b, double* d) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   double *da = nullptr, *db = nullptr, *dd = nullptr;
   PHYS_TRY(comp_ptrs(c, comp, &da, &db, &dd));
   if (c->n == 0) return PHYS_OK;
@@ -620,7 +626,7 @@ int phys_component_read(phys_ctx* c, int32_t comp, double* a, double* b, double*
 }
 
 int phys_vv_position_step(phys_ctx* c, double dt) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (c->n == 0) return fail(c, PHYS_ERR_STATE, "no body state uploaded");
   PHYS_TRY(reset_status(c));
   PHYS_TRY(verlet_drift(c, dt));
@@ -629,7 +635,7 @@ int phys_vv_position_step(phys_ctx* c, double dt) {
 }
 
 int phys_vv_velocity_step(phys_ctx* c, double dt) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (c->n == 0) return fail(c, PHYS_ERR_STATE, "no body state uploaded");
   PHYS_TRY(reset_status(c));
   PHYS_TRY(verlet_kick(c, dt));
@@ -637,7 +643,7 @@ int phys_vv_velocity_step(phys_ctx* c, double dt) {
 }
 
 int phys_gravity_forces(phys_ctx* c, const phys_params* p, double* fx, double* fy, double* fz) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   PHYS_TRY(check_params(c, p));
   if (!fx || !fy || !fz) return fail(c, PHYS_ERR_ARG, "force arrays are required");
   int64_t n = c->n;
@@ -664,7 +670,7 @@ int phys_gravity_forces(phys_ctx* c, const phys_params* p, double* fx, double* f
 }
 
 int phys_nfw_forces(phys_ctx* c, const phys_nfw_halo* halo, double* fx, double* fy, double* fz) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (!halo) return fail(c, PHYS_ERR_ARG, "halo is NULL");
   if (halo->reserved != 0) return fail(c, PHYS_ERR_ARG, "phys_nfw_halo.reserved must be 0");
   if (!halo->enabled) return PHYS_OK;  // nfw.rs:108-110
@@ -697,7 +703,7 @@ int phys_nfw_forces(phys_ctx* c, const phys_nfw_halo* halo, double* fx, double* 
 }
 
 int phys_set_nfw_halo(phys_ctx* c, const phys_nfw_halo* halo) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (halo && halo->reserved != 0) return fail(c, PHYS_ERR_ARG, "phys_nfw_halo.reserved must be 0");
   c->halo_on = halo && halo->enabled;
   if (halo) c->halo = *halo;
@@ -706,7 +712,7 @@ int phys_set_nfw_halo(phys_ctx* c, const phys_nfw_halo* halo) {
 }
 
 int phys_gravity_accel(phys_ctx* c, const phys_params* p, double* ax, double* ay, double* az) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   PHYS_TRY(check_params(c, p));
   if (c->n == 0) return fail(c, PHYS_ERR_STATE, "no body state uploaded");
   PHYS_TRY(reset_status(c));
@@ -726,7 +732,7 @@ int phys_gravity_accel(phys_ctx* c, const phys_params* p, double* ax, double* ay
 
 int phys_direct_accel_targets(phys_ctx* c, const phys_params* p, int64_t nt,
                               const int64_t* targets, double* ax, double* ay, double* az) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   PHYS_TRY(check_params(c, p));
   PHYS_TRY(positions_ready(c, false));
   if (nt < 0 || (nt > 0 && (!targets || !ax || !ay || !az)))
@@ -755,17 +761,18 @@ int phys_direct_accel_targets(phys_ctx* c, const phys_params* p, int64_t nt,
 }
 
 int phys_verlet_steps(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   return verlet_steps(c, p, dt, nsteps, true);
 }
 
 int phys_verlet_steps_async(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   return verlet_steps(c, p, dt, nsteps, false);
 }
 
 int phys_diagnostics(phys_ctx* c, double G, double* out5) {
   if (!c || !out5) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (c->n == 0) return fail(c, PHYS_ERR_STATE, "no body state uploaded");
   PHYS_TRY(positions_ready(c, false));
   return diagnostics(c, G, out5);
@@ -775,7 +782,7 @@ int phys_bh_export(phys_ctx* c, const phys_params* p, int64_t cap, int64_t* nnod
                    int32_t* depth, int64_t* count, double* mass, double* com,
                    int64_t* leaf_body, int64_t* body_leaf, uint64_t* keys_hi, uint64_t* keys_lo,
                    int64_t* perm, double* root4) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   PHYS_TRY(check_params(c, p));
   PHYS_TRY(positions_ready(c, true));
   if (c->n < 2) return fail(c, PHYS_ERR_STATE, "need at least 2 bodies");
@@ -789,16 +796,16 @@ int phys_bh_export(phys_ctx* c, const phys_params* p, int64_t cap, int64_t* nnod
 int phys_ensemble_load(phys_ctx* c, int64_t nsys, const int64_t* off, const double* x,
                        const double* y, const double* z, const double* vx, const double* vy,
                        const double* vz, const double* m) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (nsys <= 0 || !off || !x || !y || !z || !m)
     return fail(c, PHYS_ERR_ARG, "nsys > 0, offsets, positions and masses are required");
-  PHYS_CUDA(c, cudaSetDevice(c->device));
   return ensemble_load(c, nsys, off, x, y, z, vx, vy, vz, m);
 }
 
 int phys_ensemble_run(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, int32_t group,
                       int64_t chunk) {
   if (!c || !p) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (p->precision != PHYS_F64_EXACT && p->precision != PHYS_F32C)
     return fail(c, PHYS_ERR_ARG, "ensemble precision must be F64_EXACT or F32C");
   if (nsteps < 0 || chunk < 0) return fail(c, PHYS_ERR_ARG, "nsteps and chunk must be >= 0");
@@ -820,7 +827,7 @@ int phys_ensemble_run(phys_ctx* c, const phys_params* p, double dt, int64_t nste
 
 int phys_ensemble_download(phys_ctx* c, double* x, double* y, double* z, double* vx, double* vy,
                            double* vz, double* ax, double* ay, double* az) {
-  if (!c) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (c->ens_nsys <= 0) return fail(c, PHYS_ERR_STATE, "no ensemble loaded");
   return ensemble_download(c, x, y, z, vx, vy, vz, ax, ay, az);
 }
@@ -828,6 +835,7 @@ int phys_ensemble_download(phys_ctx* c, double* x, double* y, double* z, double*
 int phys_ensemble_autotune(phys_ctx* c, const phys_params* p, double dt, int64_t probe_steps,
                            int32_t* best, double* ms3) {
   if (!c || !p) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   if (probe_steps <= 0) return fail(c, PHYS_ERR_ARG, "probe_steps must be > 0");
   PHYS_TRY(reset_status(c));
   return ensemble_autotune(c, p, dt, probe_steps, best, ms3);
@@ -838,6 +846,7 @@ int phys_adjoint_direct(phys_ctx* c, const phys_params* p, double dt, int64_t ns
                         double* loss, double* gx, double* gy, double* gz, double* gvx,
                         double* gvy, double* gvz, double* gm) {
   if (!c || !loss) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   PHYS_TRY(reset_status(c));
   PHYS_TRY(positions_ready(c, false));
   PHYS_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
@@ -856,6 +865,7 @@ int phys_trajectory_loss(phys_ctx* c, const phys_params* p, double dt, int64_t n
                          const double* tx, const double* ty, const double* tz, double* loss,
                          double* xT, double* yT, double* zT) {
   if (!c || !loss) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   PHYS_TRY(reset_status(c));
   PHYS_TRY(positions_ready(c, false));
   PHYS_TRY(trajectory_loss(c, p, dt, nsteps, tx, ty, tz, loss, xT, yT, zT));
@@ -864,8 +874,15 @@ int phys_trajectory_loss(phys_ctx* c, const phys_params* p, double dt, int64_t n
   return finish_status(c);
 }
 
+int phys_debug_set_wait_limit(phys_ctx* c, int64_t spins) {
+  if (!c) return PHYS_ERR_ARG;
+  c->sort_spin_limit = spins < 0 ? (int64_t(1) << 20) : spins;
+  return PHYS_OK;
+}
+
 int phys_probe_peaks(phys_ctx* c, double* fp32, double* fp32x2, double* fp64) {
   if (!c || !fp32 || !fp32x2 || !fp64) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
   return probe_peaks(c, fp32, fp32x2, fp64);
 }
 

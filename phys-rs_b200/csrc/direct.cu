@@ -407,7 +407,8 @@ int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, 
 // with caller-provided scratch: `part` (3 * n * nslices doubles), `bh`/`bl`
 // (n float4 each, F32C only) and the status word.  Launches the same kernels
 // as direct_eval; allocates nothing.
-int direct_accel_launch_scratch(cudaStream_t s, int64_t n, const double* x, const double* y,
+cudaError_t direct_accel_launch_scratch(cudaStream_t s, int64_t n, const double* x,
+                                        const double* y,
                                 const double* z, const double* m, double G, double eps,
                                 int precision, int64_t nslices, double* part, float4* bh,
                                 float4* bl, int32_t* status, double* ox, double* oy,
@@ -427,7 +428,7 @@ int direct_accel_launch_scratch(cudaStream_t s, int64_t n, const double* x, cons
   }
   if (nsl > 1)
     slice_reduce_kernel<<<g, 256, 0, s>>>(n, (int)nsl, part, m, G, 0, ox, oy, oz, status);
-  return cudaGetLastError() == cudaSuccess ? PHYS_OK : PHYS_ERR_CUDA;
+  return cudaGetLastError();  // the launch error, if any (and clears it)
 }
 
 int direct_targets(phys_ctx* c, const phys_params* p, int64_t nt, const int64_t* d_tidx,

@@ -112,7 +112,9 @@ static_assert(kEListBytes % 32 == 0 && kEB >= kGroupMax, "evaluation kernel layo
 static_assert(kGroupMax == 64, "two targets per lane");
 static_assert(kGThrottle >= 7 * 32 + 7, "stack too small for batched pops");
 static_assert(kGThrottle + 7 * kMaxLevels + 1 <= kGStack, "stack bound");
-static_assert(kGList % 4 == 0 && kGFlushPairs % 2 == 0, "list chunks of 4 entries");
+// kGFlushPairs % 4: the split layouts (33-48-body groups) step through the
+// chunks two at a time and need an even chunk count between flushes.
+static_assert(kGList % 4 == 0 && kGFlushPairs % 4 == 0, "list chunks of 4 entries");
 static_assert((kGRecOff + 5 * 32 * 4) % 16 == 0, "record alignment");
 
 __device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
@@ -884,6 +886,7 @@ glist_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __rest
              const double4* __restrict__ body64, float theta2f, uint32_t* __restrict__ pool,
              int64_t pool_per_warp, int4* __restrict__ items, int32_t* __restrict__ nitems,
              int2* __restrict__ retry, int32_t* __restrict__ nretry, int32_t* status) {
+  if (sort_failed(status)) return;  // records built on an unfinished sort
   extern __shared__ __align__(16) unsigned char gsm[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   int* stk = reinterpret_cast<int*>(gsm) + wid * kGStack;
@@ -957,6 +960,7 @@ geval_kernel(int n, const GNode* __restrict__ gn, const int4* __restrict__ items
              const uint32_t* __restrict__ perm, double G, double eps2, int want_force,
              double* __restrict__ ox, double* __restrict__ oy, double* __restrict__ oz,
              unsigned long long* counter, int32_t* status) {
+  if (sort_failed(status)) return;  // records built on an unfinished sort
   extern __shared__ __align__(16) unsigned char gsm[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   unsigned char* lbase = gsm + wid * kESmemWarp;
@@ -996,6 +1000,7 @@ gwalk_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __rest
              double eps2, float theta2f, int want_force, double* __restrict__ ox,
              double* __restrict__ oy, double* __restrict__ oz, unsigned long long* counter,
              int32_t* status) {
+  if (sort_failed(status)) return;  // records built on an unfinished sort
   extern __shared__ __align__(16) unsigned char gsm[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   unsigned char* ws = gsm + wid * kGSmemWarp;
@@ -1097,8 +1102,9 @@ gwalk_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __rest
   }
 }
 
-// Resident blocks per SM of a kernel with its dynamic shared memory (cached
-// per kernel: its resources are fixed).
+// Resident blocks per SM of a kernel with its dynamic shared memory, and its
+// shared-memory limit raised on the context's device (cached in the context:
+// the kernel's resources are fixed).
 template <class K>
 int occupancy(phys_ctx* c, K kernel, int block, int smem, int* cache) {
   if (!*cache) {
@@ -1113,7 +1119,9 @@ int occupancy(phys_ctx* c, K kernel, int block, int smem, int* cache) {
 template <bool kF32>
 int launch(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force, double* ox,
            double* oy, double* oz) {
-  static int occ_list = 0, occ_eval = 0, occ_fused = 0;
+  int& occ_list = c->occ_gwalk[0];
+  int& occ_eval = c->occ_gwalk[kF32 ? 2 : 1];
+  int& occ_fused = c->occ_gwalk[kF32 ? 4 : 3];
   PHYS_TRY(occupancy(c, glist_kernel, kLBlock, kLSmem, &occ_list));
   PHYS_TRY(occupancy(c, geval_kernel<kF32>, kGBlock, kESmem, &occ_eval));
   PHYS_TRY(occupancy(c, gwalk_kernel<kF32>, kGBlock, kGSmem, &occ_fused));

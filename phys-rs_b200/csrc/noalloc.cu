@@ -13,6 +13,10 @@
 // the maximum problem size, kMaxBodies.  All calls share it and it keeps the
 // previous call's contents, so calls whose work overlaps on the GPU (two
 // streams, or two host threads) race on it; callers must order them.
+// The array's device address is looked up once per device and kept for the
+// life of the process; cudaDeviceReset destroys the device's context, and
+// with it the array at that address, so a process that resets a device must
+// not call this entry point on that device again.
 #include <mutex>
 
 #include "common.cuh"
@@ -65,13 +69,16 @@ extern "C" int phys_direct_accel_noalloc(int64_t n, const double* x, const doubl
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (n < 2) {  // no pairs (gravity.rs:49-51): zero accelerations
+    cudaError_t e = cudaSuccess;
     for (double* o : {ax, ay, az})
-      if (n > 0 && cudaMemsetAsync(o, 0, sizeof(double) * n, s) != cudaSuccess) {
-        set_err(errbuf, errlen, "phys_direct_accel_noalloc: %s",
-                cudaGetErrorString(cudaGetLastError()));
-        return PHYS_ERR_CUDA;
-      }
-    return cudaStreamSynchronize(s) == cudaSuccess ? PHYS_OK : PHYS_ERR_CUDA;
+      if (n > 0 && e == cudaSuccess) e = cudaMemsetAsync(o, 0, sizeof(double) * n, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      set_err(errbuf, errlen, "phys_direct_accel_noalloc: %s", cudaGetErrorString(e));
+      return PHYS_ERR_CUDA;
+    }
+    return PHYS_OK;
   }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -113,17 +120,18 @@ extern "C" int phys_direct_accel_noalloc(int64_t n, const double* x, const doubl
     set_err(errbuf, errlen, "phys_direct_accel_noalloc: %s", cudaGetErrorString(e));
     return PHYS_ERR_CUDA;
   }
-  int st = phys::direct_accel_launch_scratch(s, n, x, y, z, m, G, eps, precision, nslices, part,
-                                             bh, bl, status, ax, ay, az);
-  if (st != PHYS_OK) {
-    set_err(errbuf, errlen, "phys_direct_accel_noalloc: launch failed: %s",
-            cudaGetErrorString(cudaGetLastError()));
-    return st;
+  e = phys::direct_accel_launch_scratch(s, n, x, y, z, m, G, eps, precision, nslices, part, bh,
+                                         bl, status, ax, ay, az);
+  if (e != cudaSuccess) {
+    set_err(errbuf, errlen, "phys_direct_accel_noalloc: launch failed: %s (%s)",
+            cudaGetErrorName(e), cudaGetErrorString(e));
+    return PHYS_ERR_CUDA;
   }
   int32_t hs = 0;
   e = cudaMemcpyAsync(&hs, status, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
+    cudaGetLastError();
     set_err(errbuf, errlen, "phys_direct_accel_noalloc: %s", cudaGetErrorString(e));
     return PHYS_ERR_CUDA;
   }

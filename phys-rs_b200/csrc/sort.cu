@@ -28,7 +28,6 @@ constexpr int kMaxPasses = 8;
 constexpr uint32_t kFlagAggregate = 1u << 30;  // the tile's own digit count
 constexpr uint32_t kFlagPrefix = 2u << 30;     // count of this and every earlier tile
 constexpr uint32_t kValueMask = (1u << 30) - 1u;
-constexpr int kLookbackSpins = 1 << 20;        // bound on one digit's wait
 constexpr int kLookback = 8;                   // tiles read per look-back step
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -151,7 +150,7 @@ __global__ void __launch_bounds__(kThreads)
 radix_pass_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                   uint64_t* __restrict__ kout, uint32_t* __restrict__ vout, int64_t n, int shift,
                   const uint32_t* __restrict__ counts, uint32_t* __restrict__ status,
-                  int32_t* __restrict__ tile_ctr, int32_t* __restrict__ err) {
+                  int32_t* __restrict__ tile_ctr, int32_t* __restrict__ err, int64_t spin_limit) {
   extern __shared__ __align__(16) unsigned char ssm[];
   uint64_t* skey = reinterpret_cast<uint64_t*>(ssm);                          // kTileKeys
   uint32_t* sval = reinterpret_cast<uint32_t*>(ssm + kTileKeys * 8);          // kTileKeys
@@ -225,9 +224,14 @@ radix_pass_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__
     if (tile > 0) {
       // walk back kLookback tiles at a time (independent loads), adding
       // counts up to the nearest inclusive prefix; wait only on a tile that
-      // has not published yet (below tile 0 reads as an empty prefix)
+      // has not published yet (below tile 0 reads as an empty prefix).  A
+      // wait gives up after spin_limit re-reads: the tile raises
+      // kStatTimeout and takes the silent tile as an empty prefix, so its
+      // offsets are wrong but every write below stays inside [0, n) (the
+      // output is then no permutation; the kernels that index with it check
+      // the flag first: sort_failed in common.cuh)
       int pred = tile - 1;
-      int spins = 0;
+      int64_t spins = 0;
       bool done = false;
       while (!done) {
         uint32_t w[kLookback];
@@ -239,7 +243,7 @@ radix_pass_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__
           if (done) break;
           uint32_t x = w[j];
           while ((x & ~kValueMask) == 0) {  // not published yet
-            if (++spins > kLookbackSpins) {
+            if (++spins > spin_limit) {
               atomicOr(err, kStatTimeout);
               x = kFlagPrefix;
               break;
@@ -363,15 +367,14 @@ int radix_sort_u64(phys_ctx* c, uint64_t* keys, uint32_t* vals, uint64_t* keys_a
   if (n <= 1 || end_bit <= begin_bit) return PHYS_OK;
   if (n > (int64_t)kValueMask)
     return fail(c, PHYS_ERR_ARG, "radix sort of %lld keys: at most 2^30 - 1", (long long)n);
-  static bool smem_set = false;  // per process: the kernels' attributes are fixed
-  if (!smem_set) {
+  if (!c->sort_smem_set) {  // once per context, on its device
     PHYS_CUDA(c, cudaFuncSetAttribute(radix_pass_kernel<true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kScatterSmem));
     PHYS_CUDA(c, cudaFuncSetAttribute(radix_pass_kernel<false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kScatterSmem));
     PHYS_CUDA(c, cudaFuncSetAttribute(radix_digits_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kDigitsSmem));
-    smem_set = true;
+    c->sort_smem_set = true;
   }
   const int npass = (end_bit - begin_bit + 7) / 8;
   if (npass > kMaxPasses) return fail(c, PHYS_ERR_ARG, "radix sort over more than 64 bits");
@@ -398,10 +401,10 @@ int radix_sort_u64(phys_ctx* c, uint64_t* keys, uint32_t* vals, uint64_t* keys_a
     uint32_t* pst = status + (size_t)p * ntiles * kBins;
     if (vals) {
       PHYS_LAUNCH(c, radix_pass_kernel<true>, (int)ntiles, kThreads, kScatterSmem, ki, vi, ko, vo,
-                  n, shift, counts, pst, tile_ctr + p, c->d_status);
+                  n, shift, counts, pst, tile_ctr + p, c->d_status, c->sort_spin_limit);
     } else {
       PHYS_LAUNCH(c, radix_pass_kernel<false>, (int)ntiles, kThreads, kScatterSmem, ki, vi, ko,
-                  vo, n, shift, counts, pst, tile_ctr + p, c->d_status);
+                  vo, n, shift, counts, pst, tile_ctr + p, c->d_status, c->sort_spin_limit);
     }
     uint64_t* tk = ki;
     ki = ko;

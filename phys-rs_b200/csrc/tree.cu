@@ -168,7 +168,8 @@ __device__ __forceinline__ bool key_less(const uint64_t* klo, uint32_t a, uint32
 
 __global__ void run_fixup_kernel(int64_t n, const uint64_t* __restrict__ hs,
                                  uint32_t* __restrict__ perm, const uint64_t* __restrict__ klo,
-                                 uint32_t* __restrict__ tmp) {
+                                 uint32_t* __restrict__ tmp, const int32_t* status) {
+  if (sort_failed(status)) return;
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p + 1 < n;
        p += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t h = hs[p];
@@ -215,7 +216,8 @@ gather_sorted_kernel(int64_t n, const uint32_t* __restrict__ perm, const uint64_
                      const double* __restrict__ z, const double* __restrict__ m,
                      uint64_t* __restrict__ lo_s, double4* __restrict__ body64,
                      float4* __restrict__ body_hi, float4* __restrict__ body_lo,
-                     Body32x2* __restrict__ body2) {
+                     Body32x2* __restrict__ body2, const int32_t* status) {
+  if (sort_failed(status)) return;
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
        p += (int64_t)gridDim.x * blockDim.x) {
     const uint32_t i = perm[p];
@@ -506,7 +508,9 @@ __global__ void __launch_bounds__(kBlock)
 com_recurrence_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
                       const uint64_t* __restrict__ entries, const double* __restrict__ x,
                       const double* __restrict__ y, const double* __restrict__ z,
-                      const double* __restrict__ m, double4* __restrict__ mc) {
+                      const double* __restrict__ m, double4* __restrict__ mc,
+                      const int32_t* status) {
+  if (sort_failed(status)) return;
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnodes;
        k += (int64_t)gridDim.x * blockDim.x) {
     const int64_t e0 = eoff[k], e1 = eoff[k + 1];
@@ -619,7 +623,8 @@ __global__ void depth_key_kernel(int64_t nnodes, const int4* __restrict__ link,
 }
 
 __global__ void invert_kernel(int64_t nnodes, const uint32_t* __restrict__ bfs2pre,
-                              int32_t* __restrict__ pre2bfs) {
+                              int32_t* __restrict__ pre2bfs, const int32_t* status) {
+  if (sort_failed(status)) return;
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nnodes;
        j += (int64_t)gridDim.x * blockDim.x)
     pre2bfs[bfs2pre[j]] = (int32_t)j;
@@ -630,7 +635,8 @@ gnode_kernel(int64_t nnodes, const uint32_t* __restrict__ bfs2pre,
              const int32_t* __restrict__ pre2bfs, const int4* __restrict__ link,
              const double4* __restrict__ mc, const int32_t* __restrict__ nchild, int leaf_cap,
              const double4* __restrict__ body64, const TreeHeader* __restrict__ hdr,
-             GNode* __restrict__ g) {
+             GNode* __restrict__ g, const int32_t* status) {
+  if (sort_failed(status)) return;
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nnodes;
        j += (int64_t)gridDim.x * blockDim.x) {
     const int k = (int)bfs2pre[j];
@@ -679,7 +685,8 @@ template <bool kEmit>
 __global__ void group_kernel(int64_t nnodes, const uint32_t* __restrict__ bfs2pre,
                              const int4* __restrict__ link, const int32_t* __restrict__ nchild,
                              int32_t* __restrict__ cnt, const int32_t* __restrict__ off,
-                             int2* __restrict__ out, int64_t cap) {
+                             int2* __restrict__ out, int64_t cap, const int32_t* status) {
+  if (sort_failed(status)) return;
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j <= nnodes;
        j += (int64_t)gridDim.x * blockDim.x) {
     if (j == nnodes) {
@@ -777,18 +784,25 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
   uint64_t* hs = in_alt ? khi_alt : khi;
   uint32_t* perm = in_alt ? idx_alt : idx;
   uint32_t* spare = in_alt ? idx : idx_alt;
-  PHYS_LAUNCH(c, run_fixup_kernel, grid_for(n), kBlock, 0, n, hs, perm, klo, spare);
+  PHYS_LAUNCH(c, run_fixup_kernel, grid_for(n), kBlock, 0, n, hs, perm, klo, spare, c->d_status);
   PHYS_LAUNCH(c, gather_sorted_kernel, grid_for(n), kBlock, 0, n, perm, klo, c->x, c->y, c->z,
-              c->m, lo_s, body64, body_hi, body_lo, body2);
+              c->m, lo_s, body64, body_hi, body_lo, body2, c->d_status);
   PHYS_CUDA(c, cudaEventRecord(c->ev[5], c->stream));
   PHYS_LAUNCH(c, lcp_count_kernel, grid_for(n + 1), kBlock, 0, n, hs, lo_s, c->d_hdr, L, cnt);
   PHYS_TRY(scan_exclusive_i32(c, cnt, first, n + 1));
-  // node count + header back to the host
+  // node count, header and status word back to the host: a key sort that
+  // gave up a bounded wait ends the evaluation here, before any kernel
+  // builds on its order (the kernels between the sort and this point
+  // checked the flag themselves)
   int32_t* hsm = c->h_small;
   PHYS_CUDA(c, cudaMemcpyAsync(hsm, first + n, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
   PHYS_CUDA(c, cudaMemcpyAsync(hsm + 1, &c->d_hdr->dstar, sizeof(int32_t), cudaMemcpyDeviceToHost,
                                c->stream));
+  PHYS_CUDA(c, cudaMemcpyAsync(hsm + 2, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                               c->stream));
   PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (hsm[2] & kStatTimeout)
+    return fail(c, PHYS_ERR_TIMEOUT, "radix sort of the descent keys: a bounded wait timed out");
   int64_t nfull = hsm[0];
   const int dstar = hsm[1];
   if (nfull < 1 || nfull > (int64_t)n * (kMaxLevels + 1))
@@ -855,7 +869,7 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
     PHYS_TRY(radix_sort_u64(c, e1, nullptr, e1_alt, nullptr, total, 32, 32 + bits_n, &alt2));
     uint64_t* es = alt2 ? e1_alt : e1;
     PHYS_LAUNCH(c, com_recurrence_kernel, grid_for(nnodes, 128, 1 << 30), 128, 0, nnodes, eoff, es,
-                c->x, c->y, c->z, c->m, mc);
+                c->x, c->y, c->z, c->m, mc, c->d_status);
   } else {
     PHYS_CUDA(c, cudaMemsetAsync(arrive, 0, sizeof(int32_t) * (nnodes + 1), c->stream));
     PHYS_LAUNCH(c, com_upward_kernel, grid_for(nnodes), kBlock, 0, nnodes, link, parent, nchild,
@@ -893,9 +907,10 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
     bool alt = false;
     PHYS_TRY(radix_sort_u64(c, dk, dv, dk_alt, dv_alt, nnodes, 0, 8, &alt));
     const uint32_t* bfs2pre = alt ? dv_alt : dv;
-    PHYS_LAUNCH(c, invert_kernel, grid_for(nnodes), kBlock, 0, nnodes, bfs2pre, pre2bfs);
+    PHYS_LAUNCH(c, invert_kernel, grid_for(nnodes), kBlock, 0, nnodes, bfs2pre, pre2bfs,
+                c->d_status);
     PHYS_LAUNCH(c, gnode_kernel, grid_for(nnodes), kBlock, 0, nnodes, bfs2pre, pre2bfs, link, mc,
-                nchild, p->leaf_cap, body64, c->d_hdr, g);
+                nchild, p->leaf_cap, body64, c->d_hdr, g, c->d_status);
     t->gnode = g;
     int32_t *gcnt = nullptr, *goff = nullptr, *gctr = nullptr;
     int2* groups = nullptr;
@@ -904,10 +919,10 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
     PHYS_TRY(ws_alloc(c, WS_GROUPS, 2 * n, &groups));  // groups, then re-queued subgroups
     PHYS_TRY(ws_alloc(c, WS_GROUP_CTR, 8, &gctr));
     PHYS_LAUNCH(c, group_kernel<false>, grid_for(nnodes + 1), kBlock, 0, nnodes, bfs2pre, link,
-                nchild, gcnt, goff, groups, n);
+                nchild, gcnt, goff, groups, n, c->d_status);
     PHYS_TRY(scan_exclusive_i32(c, gcnt, goff, nnodes + 1));
     PHYS_LAUNCH(c, group_kernel<true>, grid_for(nnodes + 1), kBlock, 0, nnodes, bfs2pre, link,
-                nchild, gcnt, goff, groups, n);
+                nchild, gcnt, goff, groups, n, c->d_status);
     t->groups = groups;
     t->ngroups = goff + nnodes;
     t->group_ctr = gctr;

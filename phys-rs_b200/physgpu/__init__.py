@@ -43,7 +43,7 @@ EXPORTED = [
     "phys_direct_accel_noalloc", "phys_adjoint_direct", "phys_trajectory_loss",
     "phys_nfw_density", "phys_nfw_enclosed_mass", "phys_nfw_circular_velocity",
     "phys_nfw_forces", "phys_set_nfw_halo", "phys_state_upload_sector_state",
-    "phys_state_download_sector_state",
+    "phys_state_download_sector_state", "phys_debug_set_wait_limit",
 ]
 
 
@@ -140,6 +140,7 @@ def load_library(path=None):
                                            + [_D] * 4, ctypes.c_int),
         "phys_state_download_sector_state": ([_VP, _I64, _I64, _I64, _D, _D, _D],
                                              ctypes.c_int),
+        "phys_debug_set_wait_limit": ([_VP, i64], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -201,6 +202,12 @@ class Context:
     @property
     def stream(self):
         return self.lib.phys_ctx_stream(self.h)
+
+    def set_wait_limit(self, spins):
+        """Bound on each bounded device wait of the radix sorts (tests only);
+        a negative value restores the default."""
+        self._check(self.lib.phys_debug_set_wait_limit(self.h, int(spins)),
+                    "phys_debug_set_wait_limit")
 
     # ---- state ----
     def upload(self, pos, vel, m):
