@@ -15,7 +15,8 @@ independent system (replicas, weak scaling; the path has no exchange step);
 time is the max over ranks.  `--impl reference` times the reference's CPU
 algorithm (the C++ oracle restatement: serial pointer-octree build + threaded
 walk, two force evaluations per tick as the reference schedule runs them) on
-the host cores, rank 0 only.
+the host cores, rank 0 only: whole ticks of all N bodies, as many of the
+requested steps as fit in REFERENCE_BUDGET_S, with the count it ran.
 """
 import argparse
 import ctypes
@@ -122,11 +123,11 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def cpu_reference_tick(pos, vel, m, args, sample, rng, nthreads):
+def cpu_reference_tick_sampled(pos, vel, m, args, sample, rng, nthreads):
     """One reference Velocity-Verlet tick at full N on the host, with the
     walk timed on `sample` random targets and scaled to N (two force
-    evaluations per tick, src/main.rs:109,128).  Returns seconds per tick and
-    the parts."""
+    evaluations per tick, src/main.rs:109,128).  Used only where a full tick
+    takes minutes (the 2^24 galaxy).  Returns seconds per tick and the parts."""
     import oracle
     n = len(m)
     targets = np.sort(rng.choice(n, size=min(sample, n), replace=False))
@@ -135,7 +136,6 @@ def cpu_reference_tick(pos, vel, m, args, sample, rng, nthreads):
                                      nthreads=nthreads)
     wall = time.perf_counter() - t0
     build_s, walk_s = tm[0], tm[1] * n / len(targets)
-    # integrator systems: O(N) f64 updates, measured on the same arrays
     t1 = time.perf_counter()
     x = pos + vel * args.dt
     _ = vel + x * 0.5 * args.dt
@@ -145,43 +145,92 @@ def cpu_reference_tick(pos, vel, m, args, sample, rng, nthreads):
                                  "sample_targets": len(targets), "wall_s": wall}
 
 
+def cpu_reference_eval(pos, m, args, nthreads):
+    """One whole barnes_hut_gravity_system force evaluation of all N bodies
+    on the host: the serial pointer-octree build and the threaded walk of
+    every target (gravity_tree.rs:260-338).  Returns (seconds, build_s,
+    walk_s), all measured."""
+    import oracle
+    tm = np.zeros(2)
+    t0 = time.perf_counter()
+    oracle.bh_forces(pos, m, 1.0, args.eps, args.theta, nthreads=nthreads, timings=tm)
+    return time.perf_counter() - t0, float(tm[0]), float(tm[1])
+
+
+def cpu_reference_tick(pos, vel, m, args, nthreads):
+    """One reference Velocity-Verlet tick of all N bodies on the host, as the
+    reference schedule runs it (src/main.rs:103-140): force pass, position
+    step, force pass, velocity step, each force pass a whole Barnes-Hut
+    evaluation.  Returns the measured seconds."""
+    import oracle
+    t0 = time.perf_counter()
+    oracle.vv_run(pos, vel, m, 1.0, args.eps, args.dt, 1, method="bh", theta=args.theta,
+                  nthreads=nthreads)
+    return time.perf_counter() - t0
+
+
+# Host seconds the reference arm spends in its timed ticks: each full tick
+# of 2^20 bodies takes several seconds, so the arm runs as many of the
+# requested ticks as fit and states the number it ran.
+REFERENCE_BUDGET_S = 90.0
+
+
 def run_reference(args, ws, rank):
     import oracle
     oracle.lib()
     if rank != 0:
         return 0
     import physgpu.ics as ics
+    nthreads = oracle.ncpu()
     if args.workload == "galaxy":
         pos, vel, m = ics.galaxy(args.n, seed=0)
+        rng = np.random.default_rng(1)
+        for _ in range(args.warmup):
+            cpu_reference_tick_sampled(pos, vel, m, args, 16384, rng, nthreads)
+        ticks, parts = [], None
+        for _ in range(args.steps):
+            t, parts = cpu_reference_tick_sampled(pos, vel, m, args, 16384, rng, nthreads)
+            ticks.append(t)
+        t_tick = sum(ticks) / len(ticks)
+        steps, warmup, extra = args.steps, args.warmup, {}
+        sample = ("per tick: serial pointer-octree build of all %d bodies + threaded walk of "
+                  "%d random targets scaled to N, x2 force evaluations per tick; last tick %s" % (
+                      args.n, parts["sample_targets"],
+                      json.dumps({k: round(v, 4) for k, v in parts.items()})))
     else:
         pos, vel, m = ics.plummer(args.n, seed=0)
-    nthreads = oracle.ncpu()
-    rng = np.random.default_rng(1)
-    sample = 16384
-    for _ in range(args.warmup):
-        cpu_reference_tick(pos, vel, m, args, sample, rng, nthreads)
-    ticks, parts = [], None
-    for _ in range(args.steps):
-        t, parts = cpu_reference_tick(pos, vel, m, args, sample, rng, nthreads)
-        ticks.append(t)
-    t_tick = sum(ticks) / len(ticks)
+        # warm-up: one whole force evaluation, timed by parts
+        eval_s, build_s, walk_s = cpu_reference_eval(pos, m, args, nthreads)
+        warmup = 1
+        steps = max(1, min(args.steps, int(REFERENCE_BUDGET_S // (2.0 * eval_s))))
+        ticks = [cpu_reference_tick(pos, vel, m, args, nthreads) for _ in range(steps)]
+        t_tick = sum(ticks) / len(ticks)
+        one_eval_tick = t_tick - eval_s
+        extra = {"steps_requested": args.steps, "warmup_requested": args.warmup,
+                 "tick_s": ticks,
+                 "one_evaluation": {"eval_s": eval_s, "build_s": build_s, "walk_s": walk_s,
+                                    "tick_s": one_eval_tick,
+                                    "value": args.n / one_eval_tick,
+                                    "note": "the same tick with one force evaluation, as the "
+                                            "device path runs it (the reference schedule's two "
+                                            "passes per tick are at the same positions)"}}
+        sample = ("%d whole reference ticks of all %d bodies (serial pointer-octree build + "
+                  "threaded walk of every target, two force evaluations per tick, "
+                  "src/main.rs:109,128), each timed; no scaling" % (steps, args.n))
     value = args.n / t_tick
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": args.gpus, "steps": steps, "warmup": warmup,
         "ms_per_step": t_tick * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Plummer)",
-        "config": workload_config(args, precision="f64", leaf_cap=1),
+        "config": dict(workload_config(args, precision="f64", leaf_cap=1),
+                       l2="not applicable (host cores)"),
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": nthreads,
-                         "kind": "port",
-                         "sample": ("per tick: serial pointer-octree build of all %d bodies + "
-                                    "threaded walk of %d random targets scaled to N, x2 force "
-                                    "evaluations per tick; last tick %s" % (
-                                        args.n, parts["sample_targets"],
-                                        json.dumps({k: round(v, 4) for k, v in parts.items()})))},
+                         "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    line.update(extra)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -428,12 +477,11 @@ def run_ours(args, ws, rank, local):
         import oracle
         oracle.lib()
         nth = oracle.ncpu()
-        t_tick, parts = cpu_reference_tick(pos, vel, m, args, 16384, np.random.default_rng(1), nth)
+        t_tick = cpu_reference_tick(pos, vel, m, args, nth)
         cpu = {"value": n / t_tick, "unit": "particle-steps/s", "cores": nth, "kind": "port",
-               "sample": ("one reference tick at N=%d: serial pointer-octree build + threaded "
-                          "walk of %d targets scaled to N, x2 evaluations per tick; parts %s" % (
-                              n, parts["sample_targets"],
-                              json.dumps({k: round(v, 4) for k, v in parts.items()})))}
+               "sample": ("one whole reference tick of all %d bodies, measured: serial "
+                          "pointer-octree build + threaded walk of every target, two force "
+                          "evaluations per tick (src/main.rs:109,128); %.2f s" % (n, t_tick))}
 
     if rank == 0:
         line = {

@@ -1,0 +1,195 @@
+"""Parity at the benchmark shapes, through the C ABI, against the oracle.
+
+* 2^20-body Plummer sphere (theta 0.5, eps 0.01, leaf capacity 1 and 8):
+  descent keys, sort order and the whole octree (depth, body count, stored
+  leaf body, per-body leaf, mass and running-mean centre of mass) are
+  bit-identical to the oracle's pointer octree built by serial insertion
+  (gravity_tree.rs:110-154); PHYS_F64_EXACT forces on a 4096-target sample
+  are bit-identical to the oracle's recursive walk (gravity_tree.rs:171-234);
+  PHYS_F64 is within 1e-12 median relative of it; PHYS_F32C is within 1e-6
+  median relative of PHYS_F64 on the same tree and lists, for both walks and
+  both leaf capacities, and Barnes-Hut stays within its truncation error of
+  the f64 direct sum.
+* 2^24-body disk + NFW halo galaxy (theta 0.6, eps 0.02), group walk: F32C
+  within 1e-6 median relative of F64 on the same lists (65 536-body sample),
+  Barnes-Hut within its truncation error of the GPU f64 direct sum.
+* 16 384-system ensemble, N in [3, 64]: F64_EXACT bit-identical to the
+  oracle's per-system tick loop on 64 sampled systems after 100 steps; F32C
+  accelerations within 1e-6 median relative of F64_EXACT, positions within
+  1e-9 median relative after 100 steps.
+* Adjoint against central differences of the oracle's own forward pass (the
+  reference's Verlet tick loop and direct sum, integrators.rs:63-118,
+  gravity.rs:53-69): 64 bodies, 30 steps, h = 1e-6, 1e-5 relative."""
+import numpy as np
+import pytest
+
+import oracle
+import physgpu
+import physgpu.ics as ics
+from physgpu import BARNES_HUT, DIRECT, F32C, F64, F64_EXACT, GROUP_WALK, make_params
+
+pytestmark = pytest.mark.gpu
+
+N_C2 = 1 << 20
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b, axis=1) / np.maximum(np.linalg.norm(b, axis=1), 1e-300)
+
+
+def bh(theta, precision, leaf_cap=1, flags=0, eps=0.01):
+    return make_params(1.0, eps, theta, BARNES_HUT, precision, leaf_cap, flags)
+
+
+def dstar_of(half):
+    h, d = half, 0
+    while not (d >= 40 or h < 1e-8):
+        h *= 0.5
+        d += 1
+    return d
+
+
+@pytest.fixture(scope="module")
+def c2():
+    pos, vel, m = ics.plummer(N_C2, seed=0)
+    targets = np.sort(np.random.default_rng(1).choice(N_C2, 4096, replace=False))
+    return pos, vel, m, targets
+
+
+def test_c2_tree_keys_and_order_bitexact(ctx, c2):
+    pos, _, m, _ = c2
+    ctx.upload(pos, None, m)
+    g = ctx.bh_export(bh(0.5, F64_EXACT))
+    o = oracle.bh_export(pos, m)
+    assert np.array_equal(g["root"], o["root"])
+    assert g["nnodes"] == len(o["depth"])
+    for k in ("depth", "count", "leaf_body", "body_leaf", "mass", "com"):
+        assert np.array_equal(g[k], o[k]), k
+    hi, lo = oracle.descent_keys(pos, o["root"], dstar_of(o["root"][3]))
+    assert np.array_equal(g["keys_hi"], hi) and np.array_equal(g["keys_lo"], lo)
+    assert np.array_equal(g["perm"], np.lexsort((np.arange(N_C2), lo, hi)))
+
+
+def test_c2_f64_exact_forces_bitexact_on_sample(ctx, c2):
+    pos, _, m, t = c2
+    ctx.upload(pos, None, m)
+    f = ctx.gravity_forces(bh(0.5, F64_EXACT))
+    ref = oracle.bh_forces_targets(pos, m, 1.0, 0.01, 0.5, t)
+    assert np.array_equal(f[t], ref)
+
+
+def test_c2_f64_close_to_oracle_on_sample(ctx, c2):
+    pos, _, m, t = c2
+    ctx.upload(pos, None, m)
+    f = ctx.gravity_forces(bh(0.5, F64))
+    e = rel(f[t], oracle.bh_forces_targets(pos, m, 1.0, 0.01, 0.5, t))
+    assert np.median(e) <= 1e-12, np.median(e)
+    assert np.mean(e > 1e-9) < 2e-3  # near-tie opening flips only
+
+
+@pytest.mark.parametrize("leaf_cap,flags", [(1, 0), (8, 0), (1, GROUP_WALK), (8, GROUP_WALK)])
+def test_c2_f32c_vs_f64_same_lists_and_vs_direct(ctx, c2, leaf_cap, flags):
+    pos, _, m, t = c2
+    ctx.upload(pos, None, m)
+    a64 = ctx.gravity_accel(bh(0.5, F64, leaf_cap, flags))
+    n64 = ctx.timings()["interactions"]
+    a32 = ctx.gravity_accel(bh(0.5, F32C, leaf_cap, flags))
+    n32 = ctx.timings()["interactions"]
+    e = rel(a32, a64)
+    assert np.median(e) <= 1e-6, np.median(e)
+    assert np.quantile(e, 0.99) <= 1e-5, np.quantile(e, 0.99)
+    if flags:
+        assert n32 == n64  # the lists do not depend on the precision
+    d = ctx.direct_accel_targets(make_params(1.0, 0.01, method=DIRECT, precision=F64), t)
+    eb = rel(a32[t], d)
+    assert np.median(eb) < 1e-3, np.median(eb)  # theta = 0.5 truncation, ~3e-4
+
+
+def test_c5_galaxy_f32c_vs_f64_and_vs_direct(ctx):
+    n = 1 << 24
+    pos, _, m = ics.galaxy(n, seed=0)
+    sample = np.sort(np.random.default_rng(2).choice(n, 65536, replace=False))
+    ctx.upload(pos, None, m)
+    p64 = bh(0.6, F64, 8, GROUP_WALK, eps=0.02)
+    p32 = bh(0.6, F32C, 8, GROUP_WALK, eps=0.02)
+    a64 = ctx.gravity_accel(p64)
+    a32 = ctx.gravity_accel(p32)
+    e = rel(a32[sample], a64[sample])
+    assert np.median(e) <= 1e-6, np.median(e)
+    d = ctx.direct_accel_targets(make_params(1.0, 0.02, method=DIRECT, precision=F64),
+                                 sample[:8192])
+    eb = rel(a32[sample[:8192]], d)
+    assert np.median(eb) < 2e-2, np.median(eb)  # theta = 0.6 truncation, ~5e-3
+
+
+def test_c3_full_ensemble(ctx):
+    off, pos, vel, m = ics.ensemble(16384, seed=7)
+    dt, steps = 1e-4, 100
+    pe = make_params(1.0, 1e-3, precision=F64_EXACT)
+    p32 = make_params(1.0, 1e-3, precision=F32C)
+    ctx.ensemble_load(off, pos, vel, m)
+    ctx.ensemble_run(pe, dt, 1)
+    _, _, a1e = ctx.ensemble_download()
+    ctx.ensemble_load(off, pos, vel, m)
+    ctx.ensemble_run(p32, dt, 1)
+    _, _, a1f = ctx.ensemble_download()
+    ea = rel(a1f, a1e)
+    assert np.median(ea) <= 1e-6, np.median(ea)
+    ctx.ensemble_load(off, pos, vel, m)
+    ctx.ensemble_run(pe, dt, steps)
+    xe, ve, ae = ctx.ensemble_download()
+    ctx.ensemble_load(off, pos, vel, m)
+    ctx.ensemble_run(p32, dt, steps)
+    xf, _, _ = ctx.ensemble_download()
+    ex = rel(xf, xe)
+    assert np.median(ex) <= 1e-9, np.median(ex)
+    # 64 systems, bit for bit against the oracle's reference tick loop
+    pick = np.sort(np.random.default_rng(3).choice(16384, 64, replace=False))
+    rows = np.concatenate([np.arange(off[s], off[s + 1]) for s in pick])
+    sub_off = np.concatenate([[0], np.cumsum(off[pick + 1] - off[pick])])
+    rx, rv, ra = oracle.ensemble_run(sub_off, pos[rows], vel[rows], m[rows], 1.0, 1e-3, dt, steps)
+    assert np.array_equal(xe[rows], rx)
+    assert np.array_equal(ve[rows], rv)
+    assert np.array_equal(ae[rows], ra)
+
+
+def test_adjoint_vs_oracle_finite_differences(ctx):
+    """dL/dx0, dL/dv0 (h = 1e-6) and dL/dm (relative step 1e-3, as the
+    adjoint tests explain) of L = sum |x_i(T) - target_i|^2, the loss
+    evaluated by the oracle's reference tick loop."""
+    n, steps, dt, eps = 64, 30, 1e-3, 0.01
+    pos, vel, m = ics.plummer(n, seed=5)
+    rng = np.random.default_rng(6)
+
+    def final(P, V, M):
+        # each reference tick starts with a force pass, so the first position
+        # step uses a(x0), as the adjoint's forward pass does
+        return oracle.vv_run(P, V, M, 1.0, eps, dt, steps)[0]
+
+    targets = final(pos, vel + rng.normal(0.0, 0.01, vel.shape), m)
+
+    def loss(P, V, M):
+        return float(np.sum((final(P, V, M) - targets) ** 2))
+
+    ctx.upload(pos, vel, m)
+    L, gx, gv, gm = ctx.adjoint(make_params(1.0, eps, precision=F64), dt, steps, targets,
+                                checkpoint=8)
+    assert abs(L - loss(pos, vel, m)) <= 1e-9 * L  # FMA forward vs the reference's
+    picks = [("x", int(rng.integers(n)), int(rng.integers(3))) for _ in range(4)]
+    picks += [("v", int(rng.integers(n)), int(rng.integers(3))) for _ in range(4)]
+    picks += [("m", int(rng.integers(n)), 0) for _ in range(2)]
+    scale = {"x": np.abs(gx).max(), "v": np.abs(gv).max(), "m": np.abs(gm).max()}
+    worst = 0.0
+    for kind, i, c in picks:
+        P, V, M = pos.copy(), vel.copy(), m.copy()
+        arr = {"x": P, "v": V, "m": M}[kind]
+        idx = i if kind == "m" else (i, c)
+        h = 1e-3 * M[i] if kind == "m" else 1e-6
+        arr[idx] += h
+        lp = loss(P, V, M)
+        arr[idx] -= 2 * h
+        lm = loss(P, V, M)
+        fd = (lp - lm) / (2 * h)
+        g = {"x": gx, "v": gv, "m": gm}[kind][idx]
+        worst = max(worst, abs(fd - g) / max(abs(fd), abs(g), 1e-3 * scale[kind]))
+    assert worst < 1e-5, worst
