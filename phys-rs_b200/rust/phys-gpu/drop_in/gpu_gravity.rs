@@ -16,10 +16,15 @@
 //! evaluation per tick: the first of the reference's two passes per tick is
 //! at the positions of the previous tick's second pass, so the trajectory is
 //! the same.
+//!
+//! `gpu_energy_system` replaces compute_kinetic_energy_system and
+//! compute_potential_energy_system (src/physics/energy.rs:21-56): the
+//! O(N^2) unsoftened potential runs on the device in f64.
 use bevy_ecs::prelude::*;
 
 use crate::components::dynamics::{Acceleration, Force, Mass, PreviousAcceleration, Velocity};
 use crate::core::config::UniverseConfig;
+use crate::physics::energy::EnergyMonitor;
 use crate::core::coordinates::{LocalPosition, Sector};
 use crate::core::time::SimulationTime;
 use phys_gpu::{ffi, gravity_settings, with_thread_context, Soa3};
@@ -147,5 +152,47 @@ pub fn gpu_verlet_tick(
         acc.0.x = a.x[i];
         acc.0.y = a.y[i];
         acc.0.z = a.z[i];
+    }
+}
+
+/// Kinetic and unsoftened potential energy into the EnergyMonitor, as
+/// compute_kinetic_energy_system + compute_potential_energy_system
+/// (energy.rs:21-56: pairs with r^2 == 0 skipped), computed on the device
+/// with compensated f64 sums.
+pub fn gpu_energy_system(
+    query: Query<(&Mass, &Velocity, &Sector, &LocalPosition)>,
+    config: Res<UniverseConfig>,
+    mut monitor: ResMut<EnergyMonitor>,
+) {
+    let n = query.iter().len();
+    if n == 0 {
+        return;
+    }
+    let mut sector = [Vec::with_capacity(n), Vec::with_capacity(n), Vec::with_capacity(n)];
+    let (mut local, mut vel) = (Soa3::zeros(0), Soa3::zeros(0));
+    let mut mass = Vec::with_capacity(n);
+    for (m, v, s, l) in query.iter() {
+        sector[0].push(s.0.x);
+        sector[1].push(s.0.y);
+        sector[2].push(s.0.z);
+        local.x.push(l.0.x);
+        local.y.push(l.0.y);
+        local.z.push(l.0.z);
+        vel.x.push(v.0.x);
+        vel.y.push(v.0.y);
+        vel.z.push(v.0.z);
+        mass.push(m.0);
+    }
+    let res = with_thread_context(|gpu| {
+        gpu.upload_sectors([&sector[0], &sector[1], &sector[2]], &local, config.sector_size,
+                           false, Some(&vel), &mass)?;
+        gpu.diagnostics(config.gravitational_constant)
+    });
+    match res {
+        Ok(d) => {
+            monitor.kinetic_energy = d.kinetic;
+            monitor.potential_energy = d.potential;
+        }
+        Err(e) => eprintln!("gpu_energy_system: {e}; EnergyMonitor left unchanged"),
     }
 }
