@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--eps", type=float, default=None)
     ap.add_argument("--dt", type=float, default=None)
     ap.add_argument("--ens-steps", type=int, default=10000, help="ensemble steps per bench step")
+    ap.add_argument("--adj-steps", type=int, default=1000,
+                    help="Verlet steps per trajectory gradient (adjoint workload)")
     ap.add_argument("--no-extras", action="store_true", help="skip FP64 comparison and accuracy")
     ap.add_argument("--quick", action="store_true",
                     help="device-resident timing only (no e2e, extras, CPU baseline): profiling")
@@ -601,11 +603,12 @@ def run_other(args, ws, rank, local):
                      {"workload": "ensemble_%d_systems" % args.n, "bodies": nb_all,
                       "systems_per_rank": "split over %d rank(s) by N(N-1), no exchange" % ws,
                       "steps_per_bench_step": args.ens_steps, "eps": args.eps, "dt": args.dt,
-                      "group": best, "autotune_ms": tune,
+                      "config": best, "config_meaning": "lanes per system (1 = by size) | "
+                      "warps per block << 8", "autotune_ms": {str(k): v for k, v in tune.items()},
                       "launch": "one persistent launch per run, captured in a CUDA graph",
                       "l2": "state (%.1f MB) stays on chip for a whole run" % (nb * 80 / 1e6)},
                      interactions_per_s=pairs * args.ens_steps * args.steps / (sum(ms) * 1e-3),
-                     roofline={"kernel": "ensemble_kernel<%d>" % best, "bound": "fp32",
+                     roofline={"kernel": "ensemble_kernel (config 0x%x)" % best, "bound": "fp32",
                                "achieved": ach, "peak": max(fp32_tf, fp32x2_tf),
                                "unit": "TFLOP/s", "frac": ach / max(fp32_tf, fp32x2_tf),
                                "flops_per_interaction": 20, "traffic": None},
@@ -647,7 +650,7 @@ def run_other(args, ws, rank, local):
                      variants_ms_per_step={k: v[0] / args.steps for k, v in out.items()},
                      cpu_baseline=cpu, clocks=clk)
     elif args.workload == "adjoint":
-        n, nsteps = args.n, 1000
+        n, nsteps = args.n, args.adj_steps
         pos, vel, m = ics.plummer(n, seed=rank)
         p = make_params(1.0, args.eps, precision=F64)
         rng = np.random.default_rng(rank + 100)
@@ -662,12 +665,14 @@ def run_other(args, ws, rank, local):
         clk = clocks.stop()
         t = dist.max_over_ranks(sum(ms), device="cuda")
         value = ws * args.steps / (t * 1e-3)
-        line = _line(args, ws, "trajectory gradients/s, %d-body Plummer, 1000 VV steps, f64 "
-                     "adjoint with checkpoint 32" % n, value, "gradients/s", t / args.steps, "f64",
-                     {"workload": "adjoint_plummer_n%d_1000_steps" % n, "eps": args.eps,
+        line = _line(args, ws, "trajectory gradients/s, %d-body Plummer, %d VV steps, f64 "
+                     "adjoint with checkpoint 32" % (n, nsteps), value, "gradients/s",
+                     t / args.steps, "f64",
+                     {"workload": "adjoint_plummer_n%d_%d_steps" % (n, nsteps), "eps": args.eps,
                       "dt": args.dt, "checkpoint": 32,
-                      "work_per_gradient": "2001 force evaluations + 1001 Jacobian-vector "
-                                           "products of the direct sum"},
+                      "work_per_gradient": "%d force evaluations + %d Jacobian-vector "
+                                           "products of the direct sum" % (2 * nsteps + 1,
+                                                                           nsteps + 1)},
                      particle_steps_per_s=ws * n * nsteps * args.steps / (t * 1e-3),
                      cpu_baseline=None, clocks=clk,
                      note="the reference has no differentiation: no CPU baseline")

@@ -253,18 +253,30 @@ int phys_ensemble_load(phys_ctx* ctx, int64_t nsys, const int64_t* offsets, cons
                        const double* vz, const double* m);
 /* nsteps ticks of every system in persistent kernels (one launch per
  * `chunk` steps, 0 = all steps in one launch), the launches captured in a
- * CUDA graph.  group = lanes per system (8, 16, 32) or 0 for the autotuned
- * value (autotuning on first use).  p->precision: F64_EXACT or F32C; method
- * and theta are ignored. */
+ * CUDA graph.  `config` chooses the launch shape: lanes per system (8, 16
+ * or 32: 32 / lanes systems per warp at a time; or PHYS_ENS_BY_SIZE: 32
+ * lanes for systems of more than 16 bodies, 16 for 9..16, 8 for at most 8,
+ * a warp moving on to the smaller systems once the larger ones are taken),
+ * plus optionally PHYS_ENS_WARPS(2 or 4) warps per block (default 2); 0 =
+ * the autotuned configuration (autotuning on first use).  With 32 lanes, a
+ * system of 33..64 bodies gives every lane one target and shares the
+ * remaining targets among lane streams that each take a part of the sources.
+ * p->precision: F64_EXACT or F32C; method and theta are ignored. */
+#define PHYS_ENS_BY_SIZE 1
+#define PHYS_ENS_WARPS(w) ((w) << 8)
+#define PHYS_ENS_CANDIDATES 6
 int phys_ensemble_run(phys_ctx* ctx, const phys_params* p, double dt, int64_t nsteps,
-                      int32_t group, int64_t chunk);
+                      int32_t config, int64_t chunk);
 int phys_ensemble_download(phys_ctx* ctx, double* x, double* y, double* z, double* vx,
                            double* vy, double* vz, double* ax, double* ay, double* az);
-/* Times probe_steps steps for group sizes 8, 16, 32 from the current state
- * (restored afterwards), keeps the fastest for later runs; ms3 (optional)
- * receives the three timings. */
+/* Times probe_steps steps of each of the PHYS_ENS_CANDIDATES configurations
+ * from the current state (restored afterwards) and keeps the fastest for
+ * later runs: lanes per system 8, 16, 32 and PHYS_ENS_BY_SIZE with 2 warps
+ * per block, then 32 and PHYS_ENS_BY_SIZE with 4 warps per block, in that
+ * order.  best_config receives the chosen code; ms (optional, room for
+ * PHYS_ENS_CANDIDATES) the timings in the same order. */
 int phys_ensemble_autotune(phys_ctx* ctx, const phys_params* p, double dt, int64_t probe_steps,
-                           int32_t* best_group, double* ms3);
+                           int32_t* best_config, double* ms);
 
 /* ---- trajectory gradients (hand-written adjoint) ------------------------ */
 /* No counterpart in the reference (it has no differentiation).  Loss

@@ -80,7 +80,8 @@ struct phys_ctx {
   // ---- batched ensemble (independent small systems) ----
   int64_t ens_nsys = 0, ens_nbody = 0;
   bool ens_accel_valid = false;
-  int ens_group = 0;           // autotuned group size (0: not tuned)
+  int ens_group = 0;           // autotuned configuration code (0: not tuned)
+  int64_t ens_n32 = 0, ens_n16 = 0;  // systems (sorted by size) with > 16 and > 8 bodies
 
   // ---- per-device launch data, kept per context ----
   // A kernel's dynamic shared-memory limit (cudaFuncSetAttribute) is set on

@@ -802,8 +802,8 @@ int phys_ensemble_load(phys_ctx* c, int64_t nsys, const int64_t* off, const doub
   return ensemble_load(c, nsys, off, x, y, z, vx, vy, vz, m);
 }
 
-int phys_ensemble_run(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, int32_t group,
-                      int64_t chunk) {
+int phys_ensemble_run(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps,
+                      int32_t group, int64_t chunk) {
   if (!c || !p) return PHYS_ERR_ARG;
   PHYS_ENTER(c);
   if (p->precision != PHYS_F64_EXACT && p->precision != PHYS_F32C)

@@ -20,19 +20,27 @@ namespace phys {
 namespace {
 
 constexpr int kMaxSys = 64;        // bodies per system
-constexpr int kEnsBlock = 64;      // threads per block
+constexpr int kEnsCandidates = PHYS_ENS_CANDIDATES;
 
-struct GroupSmem {
-  double x[kMaxSys], y[kMaxSys], z[kMaxSys];
-  double vx[kMaxSys], vy[kMaxSys], vz[kMaxSys];
-  double ax[kMaxSys], ay[kMaxSys], az[kMaxSys];
-  double pax[kMaxSys], pay[kMaxSys], paz[kMaxSys];
-  double m[kMaxSys];
+// Per-group state in shared memory for systems of at most MAXN bodies.
+template <int MAXN>
+struct GroupSmemT {
+  double x[MAXN], y[MAXN], z[MAXN];
+  double vx[MAXN], vy[MAXN], vz[MAXN];
+  double ax[MAXN], ay[MAXN], az[MAXN];
+  double pax[MAXN], pay[MAXN], paz[MAXN];
+  double m[MAXN];
   // F32C staging, structure of arrays so that a float2 load gives two
   // consecutive bodies (slot N of an odd-N system is a massless pad far away)
-  float hx[kMaxSys], hy[kMaxSys], hz[kMaxSys], hm[kMaxSys];  // hi parts, m (f32)
-  float lx[kMaxSys], ly[kMaxSys], lz[kMaxSys];               // lo parts
+  float hx[MAXN], hy[MAXN], hz[MAXN], hm[MAXN];  // hi parts, m (f32)
+  float lx[MAXN], ly[MAXN], lz[MAXN];            // lo parts
 };
+using GroupSmem = GroupSmemT<kMaxSys>;
+// With lanes per system chosen by size, a warp's shared memory holds one
+// 64-body group, two 16-body groups or four 8-body groups in turn.
+static_assert(2 * sizeof(GroupSmemT<16>) <= sizeof(GroupSmem) &&
+                  4 * sizeof(GroupSmemT<8>) <= sizeof(GroupSmem),
+              "sub-warp groups fit in a warp's share");
 
 template <int G>
 __device__ __forceinline__ unsigned group_mask() {
@@ -44,14 +52,16 @@ __device__ __forceinline__ unsigned group_mask() {
   }
 }
 
-__device__ __forceinline__ void split_into(GroupSmem* S, int i) {
+template <class S_t>
+__device__ __forceinline__ void split_into(S_t* S, int i) {
   split_df(S->x[i], S->hx[i], S->lx[i]);
   split_df(S->y[i], S->hy[i], S->ly[i]);
   split_df(S->z[i], S->hz[i], S->lz[i]);
   S->hm[i] = (float)S->m[i];
 }
 
-__device__ __forceinline__ void set_pad(GroupSmem* S, int i) {
+template <class S_t>
+__device__ __forceinline__ void set_pad(S_t* S, int i) {
   S->hx[i] = S->hy[i] = S->hz[i] = 1e15f;
   S->hm[i] = S->lx[i] = S->ly[i] = S->lz[i] = 0.f;
 }
@@ -60,12 +70,48 @@ __device__ __forceinline__ float2 ld2(const float* p) {
   return *reinterpret_cast<const float2*>(p);
 }
 
+// One source pair (bodies j, j + 1) against one target; skip0 / skip1 zero
+// the half that is the target itself (i == j is skipped, gravity.rs:56).
+struct PairSrc {
+  float2 sx, sy, sz, sm, tx, ty, tz;
+};
+template <class S_t>
+__device__ __forceinline__ PairSrc load_pair(const S_t* S, int j) {
+  return PairSrc{ld2(S->hx + j), ld2(S->hy + j), ld2(S->hz + j), ld2(S->hm + j),
+                 ld2(S->lx + j), ld2(S->ly + j), ld2(S->lz + j)};
+}
+__device__ __forceinline__ void pair_term(const PairSrc& s, float2 nhx, float2 nhy, float2 nhz,
+                                          float2 nlx, float2 nly, float2 nlz, float2 e2,
+                                          bool skip0, bool skip1, float2& px, float2& py,
+                                          float2& pz) {
+  const float2 rx = __fadd2_rn(__fadd2_rn(s.sx, nhx), __fadd2_rn(s.tx, nlx));
+  const float2 ry = __fadd2_rn(__fadd2_rn(s.sy, nhy), __fadd2_rn(s.ty, nly));
+  const float2 rz = __fadd2_rn(__fadd2_rn(s.sz, nhz), __fadd2_rn(s.tz, nlz));
+  const float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, e2)));
+  const float2 inv = make_float2(rsqrt_sfu(r2.x), rsqrt_sfu(r2.y));
+  float2 w = __fmul2_rn(s.sm, __fmul2_rn(__fmul2_rn(inv, inv), inv));
+  if (skip0) w.x = 0.f;
+  if (skip1) w.y = 0.f;
+  px = __ffma2_rn(rx, w, px);
+  py = __ffma2_rn(ry, w, py);
+  pz = __ffma2_rn(rz, w, pz);
+}
+
+// Folds packed partial sums into a (hi, lo) accumulator by two-sum.
+__device__ __forceinline__ void fold(float2& p, float& h, float& l) {
+  float s, e;
+  two_sum(h, p.x + p.y, s, e);
+  h = s;
+  l += e;
+  p = make_float2(0.f, 0.f);
+}
+
 // F32C accelerations of the group's own targets, TC targets per pass.  Two
 // sources per packed f32x2 operation (bodies j, j+1; an odd N reads the pad
 // at slot N); partial sums of 16 sources folded into a (hi, lo) accumulator
 // by two-sum.
-template <int G, int TC>
-__device__ void group_forces_f32c(GroupSmem* S, int N, int gl, double Gc, float eps2f) {
+template <int G, int TC, class S_t>
+__device__ void group_forces_f32c(S_t* S, int N, int gl, double Gc, float eps2f) {
   const float2 e2 = make_float2(eps2f, eps2f);
   for (int i0 = gl; i0 < N; i0 += G * TC) {
     float2 nhx[TC], nhy[TC], nhz[TC], nlx[TC], nly[TC], nlz[TC], px[TC], py[TC], pz[TC];
@@ -87,31 +133,17 @@ __device__ void group_forces_f32c(GroupSmem* S, int N, int gl, double Gc, float 
     for (int j0 = 0; j0 < N; j0 += 16) {
       const int j1 = min(N, j0 + 16);
       for (int j = j0; j < j1; j += 2) {
-        const float2 sx = ld2(S->hx + j), sy = ld2(S->hy + j), sz = ld2(S->hz + j);
-        const float2 sm = ld2(S->hm + j);
-        const float2 tx = ld2(S->lx + j), ty = ld2(S->ly + j), tz = ld2(S->lz + j);
+        const PairSrc s = load_pair(S, j);
 #pragma unroll
-        for (int t = 0; t < TC; ++t) {
-          const float2 rx = __fadd2_rn(__fadd2_rn(sx, nhx[t]), __fadd2_rn(tx, nlx[t]));
-          const float2 ry = __fadd2_rn(__fadd2_rn(sy, nhy[t]), __fadd2_rn(ty, nly[t]));
-          const float2 rz = __fadd2_rn(__fadd2_rn(sz, nhz[t]), __fadd2_rn(tz, nlz[t]));
-          const float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, e2)));
-          const float2 inv = make_float2(rsqrt_sfu(r2.x), rsqrt_sfu(r2.y));
-          float2 w = __fmul2_rn(sm, __fmul2_rn(__fmul2_rn(inv, inv), inv));
-          if (j == idx[t]) w.x = 0.f;       // self (i == j skipped, gravity.rs:56)
-          if (j + 1 == idx[t]) w.y = 0.f;
-          px[t] = __ffma2_rn(rx, w, px[t]);
-          py[t] = __ffma2_rn(ry, w, py[t]);
-          pz[t] = __ffma2_rn(rz, w, pz[t]);
-        }
+        for (int t = 0; t < TC; ++t)
+          pair_term(s, nhx[t], nhy[t], nhz[t], nlx[t], nly[t], nlz[t], e2, j == idx[t],
+                    j + 1 == idx[t], px[t], py[t], pz[t]);
       }
 #pragma unroll
       for (int t = 0; t < TC; ++t) {
-        float s, e;
-        two_sum(hx[t], px[t].x + px[t].y, s, e); hx[t] = s; lx[t] += e;
-        two_sum(hy[t], py[t].x + py[t].y, s, e); hy[t] = s; ly[t] += e;
-        two_sum(hz[t], pz[t].x + pz[t].y, s, e); hz[t] = s; lz[t] += e;
-        px[t] = py[t] = pz[t] = make_float2(0.f, 0.f);
+        fold(px[t], hx[t], lx[t]);
+        fold(py[t], hy[t], ly[t]);
+        fold(pz[t], hz[t], lz[t]);
       }
     }
 #pragma unroll
@@ -125,9 +157,88 @@ __device__ void group_forces_f32c(GroupSmem* S, int N, int gl, double Gc, float 
   }
 }
 
+__device__ __forceinline__ int next_pow2(int v) {
+  int p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+// F32C forces of a 33..64-body system on one warp without idle second
+// slots: lane l takes target a = l over every source pair, and one of the
+// nb = N - 32 second targets, b = 32 + l mod lps (lps = nb rounded up to a
+// power of two), over its stream's share of the source pairs: the warp's
+// r = 32 / lps streams take alternate pairs, and their sums for the same b
+// are added by shuffles at the end.  Each round covers r source pairs: all r
+// against a, one (the stream's own) against b.
+template <class S_t>
+__device__ void group_forces_f32c_split(S_t* S, int N, int gl, double Gc, float eps2f) {
+  const float2 e2 = make_float2(eps2f, eps2f);
+  const int nb = N - 32;
+  const int lps = next_pow2(nb), r = 32 / lps;
+  const int st = gl / lps, tb = 32 + gl % lps;
+  const int ta = gl;
+  const int tbv = tb < N ? tb : ta;  // lanes without a valid b compute a dummy (discarded)
+  auto neg = [](float v) { return make_float2(-v, -v); };
+  const float2 ahx = neg(S->hx[ta]), ahy = neg(S->hy[ta]), ahz = neg(S->hz[ta]);
+  const float2 alx = neg(S->lx[ta]), aly = neg(S->ly[ta]), alz = neg(S->lz[ta]);
+  const float2 bhx = neg(S->hx[tbv]), bhy = neg(S->hy[tbv]), bhz = neg(S->hz[tbv]);
+  const float2 blx = neg(S->lx[tbv]), bly = neg(S->ly[tbv]), blz = neg(S->lz[tbv]);
+  float2 pax = make_float2(0.f, 0.f), pay = pax, paz = pax, pbx = pax, pby = pax, pbz = pax;
+  float hax = 0.f, hay = 0.f, haz = 0.f, lax = 0.f, lay = 0.f, laz = 0.f;
+  float hbx = 0.f, hby = 0.f, hbz = 0.f, lbx = 0.f, lby = 0.f, lbz = 0.f;
+  const int npairs = (N + 1) >> 1;
+  int fa = 0, fb = 0;  // pairs in the partial sums
+  for (int q = 0; q < npairs; q += r) {
+    for (int k = 0; k < r && q + k < npairs; ++k) {
+      const int j = 2 * (q + k);
+      pair_term(load_pair(S, j), ahx, ahy, ahz, alx, aly, alz, e2, j == ta, j + 1 == ta, pax,
+                pay, paz);
+      if (++fa == 8) {
+        fold(pax, hax, lax);
+        fold(pay, hay, lay);
+        fold(paz, haz, laz);
+        fa = 0;
+      }
+    }
+    const int pb = q + st;
+    if (pb < npairs) {
+      const int j = 2 * pb;
+      pair_term(load_pair(S, j), bhx, bhy, bhz, blx, bly, blz, e2, j == tbv, j + 1 == tbv, pbx,
+                pby, pbz);
+      if (++fb == 8) {
+        fold(pbx, hbx, lbx);
+        fold(pby, hby, lby);
+        fold(pbz, hbz, lbz);
+        fb = 0;
+      }
+    }
+  }
+  fold(pax, hax, lax);
+  fold(pay, hay, lay);
+  fold(paz, haz, laz);
+  fold(pbx, hbx, lbx);
+  fold(pby, hby, lby);
+  fold(pbz, hbz, lbz);
+  S->ax[ta] = Gc * ((double)hax + (double)lax);
+  S->ay[ta] = Gc * ((double)hay + (double)lay);
+  S->az[ta] = Gc * ((double)haz + (double)laz);
+  double bx = (double)hbx + (double)lbx, by = (double)hby + (double)lby,
+         bz = (double)hbz + (double)lbz;
+  for (int o = lps; o < 32; o <<= 1) {  // the streams' sums of the same b
+    bx += __shfl_xor_sync(0xffffffffu, bx, o);
+    by += __shfl_xor_sync(0xffffffffu, by, o);
+    bz += __shfl_xor_sync(0xffffffffu, bz, o);
+  }
+  if (st == 0 && tb < N) {
+    S->ax[tb] = Gc * bx;
+    S->ay[tb] = Gc * by;
+    S->az[tb] = Gc * bz;
+  }
+}
+
 // Accelerations of the group's own targets (i = gl, gl+G, ...) into S->a.
-template <int G, bool kExact>
-__device__ void group_forces(GroupSmem* S, int N, int gl, double Gc, double eps2) {
+template <int G, bool kExact, class S_t>
+__device__ void group_forces(S_t* S, int N, int gl, double Gc, double eps2) {
   if (kExact) {
     for (int i = gl; i < N; i += G) {
       const double xi = S->x[i], yi = S->y[i], zi = S->z[i], mi = S->m[i];
@@ -148,62 +259,75 @@ __device__ void group_forces(GroupSmem* S, int N, int gl, double Gc, double eps2
     }
     return;
   }
-  // targets per lane for this system: 1, 2 or (up to 8 in passes of) 4
   const float eps2f = (float)eps2;
+  if (G == 32 && N > 32) {
+    group_forces_f32c_split(S, N, gl, Gc, eps2f);
+    return;
+  }
+  // targets per lane for this system: 1, 2 or (up to 8 in passes of) 4
   const int tpl = (N + G - 1) / G;
   if (tpl <= 1)
     group_forces_f32c<G, 1>(S, N, gl, Gc, eps2f);
-  else if (tpl == 2 || G == 32)
+  else if (tpl == 2)
     group_forces_f32c<G, 2>(S, N, gl, Gc, eps2f);
   else
     group_forces_f32c<G, 4>(S, N, gl, Gc, eps2f);
 }
 
-template <int G, bool kExact>
-__global__ void __launch_bounds__(kEnsBlock)
-ensemble_kernel(int nsys, const int32_t* __restrict__ order, const int64_t* __restrict__ off,
-                double* __restrict__ x, double* __restrict__ y, double* __restrict__ z,
-                double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
-                double* __restrict__ ax, double* __restrict__ ay, double* __restrict__ az,
-                const double* __restrict__ m, double Gc, double eps2, double dt, int nsteps,
-                int need_accel, int* queue, int32_t* status) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int gid = threadIdx.x / G, gl = threadIdx.x % G;
-  GroupSmem* S = reinterpret_cast<GroupSmem*>(smem_raw) + gid;
+struct EnsArgs {
+  int nsys;
+  const int32_t* order;
+  const int64_t* off;
+  double *x, *y, *z, *vx, *vy, *vz, *ax, *ay, *az;
+  const double* m;
+  double Gc, eps2, dt;
+  int nsteps, need_accel;
+  int* queue;      // three work counters of this launch
+  int32_t* status;
+  int n32, n16;    // by-size mode: systems [0, n32) have > 16 bodies, [n32, n16) 9..16
+};
+
+// A group of G lanes takes systems s in [lo, hi) from the counter and runs
+// `nsteps` reference ticks on each with its state in shared memory.
+template <int G, bool kExact, class S_t>
+__device__ void drain(S_t* S, const EnsArgs& a, int lo, int hi, int* ctr, int maxn) {
+  const int gl = (threadIdx.x & 31) % G;
   const unsigned gm = group_mask<G>();
+  const double dt = a.dt;
   const double h2 = xmul(xmul(0.5, dt), dt), hdt = xmul(0.5, dt);
   for (;;) {
     int s = 0;
-    if (gl == 0) s = atomicAdd(queue, 1);
+    if (gl == 0) s = lo + atomicAdd(ctr, 1);
     s = __shfl_sync(gm, s, 0, G);
-    if (s >= nsys) break;
-    const int sys = order[s];
-    const int64_t b = off[sys];
-    const int N = (int)(off[sys + 1] - b);
-    if (N > kMaxSys || N < 0) {
-      if (gl == 0) atomicOr(status, kStatOverflow);
+    if (s >= hi) break;
+    const int sys = a.order[s];
+    const int64_t b = a.off[sys];
+    const int N = (int)(a.off[sys + 1] - b);
+    // odd N uses slot N as a pad: N < maxn, or N == maxn when even
+    if (N < 0 || N > maxn || ((N & 1) && N == maxn)) {
+      if (gl == 0) atomicOr(a.status, kStatOverflow);
       continue;
     }
     for (int i = gl; i < N; i += G) {
-      S->x[i] = x[b + i];
-      S->y[i] = y[b + i];
-      S->z[i] = z[b + i];
-      S->vx[i] = vx[b + i];
-      S->vy[i] = vy[b + i];
-      S->vz[i] = vz[b + i];
-      S->ax[i] = ax[b + i];
-      S->ay[i] = ay[b + i];
-      S->az[i] = az[b + i];
-      S->m[i] = m[b + i];
+      S->x[i] = a.x[b + i];
+      S->y[i] = a.y[b + i];
+      S->z[i] = a.z[b + i];
+      S->vx[i] = a.vx[b + i];
+      S->vy[i] = a.vy[b + i];
+      S->vz[i] = a.vz[b + i];
+      S->ax[i] = a.ax[b + i];
+      S->ay[i] = a.ay[b + i];
+      S->az[i] = a.az[b + i];
+      S->m[i] = a.m[b + i];
       split_into(S, i);
     }
-    if ((N & 1) && gl == 0) set_pad(S, N);  // N <= kMaxSys - 1 here
+    if ((N & 1) && gl == 0) set_pad(S, N);
     __syncwarp(gm);
-    if (need_accel && N >= 2) group_forces<G, kExact>(S, N, gl, Gc, eps2);
-    if (need_accel && N < 2)
+    if (a.need_accel && N >= 2) group_forces<G, kExact>(S, N, gl, a.Gc, a.eps2);
+    if (a.need_accel && N < 2)
       for (int i = gl; i < N; i += G) S->ax[i] = S->ay[i] = S->az[i] = 0.0;
     __syncwarp(gm);
-    for (int st = 0; st < nsteps; ++st) {
+    for (int st = 0; st < a.nsteps; ++st) {
       // velocity_verlet_position_system: prev = a; x += v dt + a dt^2/2
       for (int i = gl; i < N; i += G) {
         const double a0 = S->ax[i], a1 = S->ay[i], a2 = S->az[i];
@@ -216,7 +340,7 @@ ensemble_kernel(int nsys, const int32_t* __restrict__ order, const int64_t* __re
         split_into(S, i);
       }
       __syncwarp(gm);
-      if (N >= 2) group_forces<G, kExact>(S, N, gl, Gc, eps2);
+      if (N >= 2) group_forces<G, kExact>(S, N, gl, a.Gc, a.eps2);
       __syncwarp(gm);
       // velocity_verlet_velocity_system: v += (prev + a) dt/2
       for (int i = gl; i < N; i += G) {
@@ -228,39 +352,58 @@ ensemble_kernel(int nsys, const int32_t* __restrict__ order, const int64_t* __re
     }
     bool bad = false;
     for (int i = gl; i < N; i += G) {
-      x[b + i] = S->x[i];
-      y[b + i] = S->y[i];
-      z[b + i] = S->z[i];
-      vx[b + i] = S->vx[i];
-      vy[b + i] = S->vy[i];
-      vz[b + i] = S->vz[i];
-      ax[b + i] = S->ax[i];
-      ay[b + i] = S->ay[i];
-      az[b + i] = S->az[i];
+      a.x[b + i] = S->x[i];
+      a.y[b + i] = S->y[i];
+      a.z[b + i] = S->z[i];
+      a.vx[b + i] = S->vx[i];
+      a.vy[b + i] = S->vy[i];
+      a.vz[b + i] = S->vz[i];
+      a.ax[b + i] = S->ax[i];
+      a.ay[b + i] = S->ay[i];
+      a.az[b + i] = S->az[i];
       bad |= !isfinite(S->x[i]) || !isfinite(S->vx[i]) || !isfinite(S->ax[i]);
     }
-    if (bad) atomicOr(status, kStatNonfinite);
+    if (bad) atomicOr(a.status, kStatNonfinite);
     __syncwarp(gm);
   }
 }
 
-using EnsKernel = void (*)(int, const int32_t*, const int64_t*, double*, double*, double*,
-                           double*, double*, double*, double*, double*, double*, const double*,
-                           double, double, double, int, int, int*, int32_t*);
+// One persistent launch of BW warps per block.  G = 8, 16, 32: every system
+// gets G lanes (32 / G systems per warp at a time).  G = 0: lanes by size —
+// a warp takes the systems of more than 16 bodies one at a time, then two of
+// 9..16 bodies at a time (16 lanes each), then four of at most 8.
+template <int G, int BW, bool kExact>
+__global__ void __launch_bounds__(32 * BW)
+ensemble_kernel(EnsArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if constexpr (G != 0) {
+    GroupSmem* S = reinterpret_cast<GroupSmem*>(smem_raw) + warp * (32 / G) + lane / G;
+    drain<G, kExact>(S, a, 0, a.nsys, a.queue, kMaxSys);
+  } else {
+    unsigned char* base = smem_raw + warp * sizeof(GroupSmem);
+    drain<32, kExact>(reinterpret_cast<GroupSmem*>(base), a, 0, a.n32, a.queue, kMaxSys);
+    drain<16, kExact>(reinterpret_cast<GroupSmemT<16>*>(base) + (lane >> 4), a, a.n32, a.n16,
+                      a.queue + 1, 16);
+    drain<8, kExact>(reinterpret_cast<GroupSmemT<8>*>(base) + (lane >> 3), a, a.n16, a.nsys,
+                     a.queue + 2, 8);
+  }
+}
 
-EnsKernel pick(int G, bool exact) {
-  if (exact) {
-    switch (G) {
-      case 8: return ensemble_kernel<8, true>;
-      case 16: return ensemble_kernel<16, true>;
-      default: return ensemble_kernel<32, true>;
-    }
-  }
+using EnsKernel = void (*)(EnsArgs);
+
+template <int BW>
+EnsKernel pick_bw(int G, bool exact) {
   switch (G) {
-    case 8: return ensemble_kernel<8, false>;
-    case 16: return ensemble_kernel<16, false>;
-    default: return ensemble_kernel<32, false>;
+    case 8: return exact ? ensemble_kernel<8, BW, true> : ensemble_kernel<8, BW, false>;
+    case 16: return exact ? ensemble_kernel<16, BW, true> : ensemble_kernel<16, BW, false>;
+    case 32: return exact ? ensemble_kernel<32, BW, true> : ensemble_kernel<32, BW, false>;
+    default: return exact ? ensemble_kernel<0, BW, true> : ensemble_kernel<0, BW, false>;
   }
+}
+
+EnsKernel pick(int G, int bw, bool exact) {
+  return bw == 4 ? pick_bw<4>(G, exact) : pick_bw<2>(G, exact);
 }
 
 struct EnsView {
@@ -278,23 +421,41 @@ struct LaunchCfg {
   EnsKernel k;
   size_t smem;
   int64_t grid;
+  int block;
 };
 
+// Launch configuration code: lanes per system (8, 16, 32 or
+// PHYS_ENS_BY_SIZE) | warps per block << 8 (2 or 4; 0 means 2).
+bool decode(int code, int* G, int* bw) {
+  const int g = code & 0xff, w = (code >> 8) & 0xff;
+  if (code & ~0xffff) return false;
+  if (g != 8 && g != 16 && g != 32 && g != PHYS_ENS_BY_SIZE) return false;
+  if (w != 0 && w != 2 && w != 4) return false;
+  *G = g == PHYS_ENS_BY_SIZE ? 0 : g;
+  *bw = w == 0 ? 2 : w;
+  return true;
+}
+
 // Kernel attributes and the persistent grid size (queried outside capture).
-int prepare(phys_ctx* c, const phys_params* p, int G, LaunchCfg* cfg) {
+int prepare(phys_ctx* c, const phys_params* p, int code, LaunchCfg* cfg) {
+  int G = 0, bw = 2;
+  if (!decode(code, &G, &bw)) return fail(c, PHYS_ERR_ARG, "ensemble configuration 0x%x", code);
   const bool exact = p->precision == PHYS_F64_EXACT;
-  cfg->k = pick(G, exact);
-  cfg->smem = sizeof(GroupSmem) * (kEnsBlock / G);
+  cfg->k = pick(G, bw, exact);
+  cfg->block = 32 * bw;
+  const int groups_per_warp = G == 0 ? 1 : 32 / G;
+  cfg->smem = sizeof(GroupSmem) * groups_per_warp * bw;
   PHYS_CUDA(c, cudaFuncSetAttribute(cfg->k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)cfg->smem));
   int per_sm = 0;
-  PHYS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg->k, kEnsBlock,
+  PHYS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg->k, cfg->block,
                                                              cfg->smem));
   int sms = 148;
   PHYS_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-  const int groups_per_block = kEnsBlock / G;
+  const int64_t groups_per_block = (int64_t)groups_per_warp * bw;
   cfg->grid = std::min<int64_t>((int64_t)std::max(per_sm, 1) * sms,
                                 ceil_div(c->ens_nsys, groups_per_block));
+  if (cfg->grid < 1) cfg->grid = 1;
   return PHYS_OK;
 }
 
@@ -303,22 +464,35 @@ int enqueue_run(phys_ctx* c, const phys_params* p, const LaunchCfg& cfg, double 
                 int64_t nsteps, int64_t chunk, bool need_accel_first) {
   EnsView v = view(c);
   int* queue = reinterpret_cast<int*>(c->ws[WS_ENS3].p);
-  const double eps2 = p->eps * p->eps;
+  EnsArgs a;
+  a.nsys = (int)c->ens_nsys;
+  a.order = reinterpret_cast<const int32_t*>(c->ws[WS_ENS2].p);
+  a.off = reinterpret_cast<const int64_t*>(c->ws[WS_ENS1].p);
+  a.x = v.x; a.y = v.y; a.z = v.z;
+  a.vx = v.vx; a.vy = v.vy; a.vz = v.vz;
+  a.ax = v.ax; a.ay = v.ay; a.az = v.az;
+  a.m = v.m;
+  a.Gc = p->G;
+  a.eps2 = p->eps * p->eps;
+  a.dt = dt;
+  a.status = c->d_status;
+  a.n32 = (int)c->ens_n32;
+  a.n16 = (int)c->ens_n16;
   int64_t done = 0;
   int ci = 0;
   bool need = need_accel_first;
   do {
     const int64_t k_steps = std::min<int64_t>(chunk, nsteps - done);
-    PHYS_CUDA(c, cudaMemsetAsync(queue + ci, 0, sizeof(int), c->stream));
-    cfg.k<<<(unsigned)cfg.grid, kEnsBlock, cfg.smem, c->stream>>>(
-        (int)c->ens_nsys, reinterpret_cast<const int32_t*>(c->ws[WS_ENS2].p),
-        reinterpret_cast<const int64_t*>(c->ws[WS_ENS1].p), v.x, v.y, v.z, v.vx, v.vy, v.vz, v.ax,
-        v.ay, v.az, v.m, p->G, eps2, dt, (int)k_steps, need ? 1 : 0, queue + ci, c->d_status);
+    a.queue = queue + 4 * ci;  // three counters per launch
+    a.nsteps = (int)k_steps;
+    a.need_accel = need ? 1 : 0;
+    PHYS_CUDA(c, cudaMemsetAsync(a.queue, 0, 4 * sizeof(int), c->stream));
+    cfg.k<<<(unsigned)cfg.grid, cfg.block, cfg.smem, c->stream>>>(a);
     c->launches++;
     PHYS_TRY(check_launch(c, "ensemble_kernel"));
     need = false;
     done += k_steps;
-    ci = (ci + 1) & 1023;
+    ci = (ci + 1) & 255;
   } while (done < nsteps);
   return PHYS_OK;
 }
@@ -353,6 +527,15 @@ int ensemble_load(phys_ctx* c, int64_t nsys, const int64_t* off, const double* x
   if (st) return st;
   c->ens_nsys = nsys;
   c->ens_nbody = n;
+  // by-size launches: the sorted systems with more than 16, then 9..16 bodies
+  int64_t n32 = 0, n16 = 0;
+  for (int64_t s = 0; s < nsys; ++s) {
+    const int64_t k = off[order[s] + 1] - off[order[s]];
+    n32 += k > 16;
+    n16 += k > 8;
+  }
+  c->ens_n32 = n32;
+  c->ens_n16 = n16;
   c->ens_accel_valid = false;
   EnsView v = view(c);
   const double* src[7] = {x, y, z, vx, vy, vz, m};
@@ -375,9 +558,8 @@ int ensemble_load(phys_ctx* c, int64_t nsys, const int64_t* off, const double* x
 }
 
 int ensemble_run(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, int G,
-                 int64_t chunk) {
+                 int64_t chunk) {  // G: configuration code
   if (c->ens_nsys <= 0) return fail(c, PHYS_ERR_STATE, "no ensemble loaded");
-  if (G != 8 && G != 16 && G != 32) return fail(c, PHYS_ERR_ARG, "group size must be 8, 16 or 32");
   if (chunk <= 0) chunk = nsteps > 0 ? nsteps : 1;
   LaunchCfg cfg;
   PHYS_TRY(prepare(c, p, G, &cfg));
@@ -419,10 +601,16 @@ int ensemble_download(phys_ctx* c, double* x, double* y, double* z, double* vx, 
   return PHYS_OK;
 }
 
-// Times `probe_steps` steps for each group size from the same starting state
-// (saved and restored around the probes) and keeps the fastest.
+// Times `probe_steps` steps for each candidate configuration from the same
+// starting state (saved and restored around the probes) and keeps the
+// fastest.  The candidates: lanes per system 8, 16, 32 and by size, two
+// warps per block; 32 and by size, four warps per block.
+const int kTuneCand[kEnsCandidates] = {8 | 2 << 8, 16 | 2 << 8, 32 | 2 << 8,
+                                       PHYS_ENS_BY_SIZE | 2 << 8, 32 | 4 << 8,
+                                       PHYS_ENS_BY_SIZE | 4 << 8};
+
 int ensemble_autotune(phys_ctx* c, const phys_params* p, double dt, int64_t probe_steps,
-                      int32_t* best, double* ms3) {
+                      int32_t* best, double* ms_out) {
   if (c->ens_nsys <= 0) return fail(c, PHYS_ERR_STATE, "no ensemble loaded");
   const int64_t n = c->ens_nbody;
   int st = PHYS_OK;
@@ -432,26 +620,25 @@ int ensemble_autotune(phys_ctx* c, const phys_params* p, double dt, int64_t prob
   const bool valid0 = c->ens_accel_valid;
   PHYS_CUDA(c, cudaMemcpyAsync(save, v.x, sizeof(double) * 9 * n, cudaMemcpyDeviceToDevice,
                                c->stream));
-  const int cand[3] = {8, 16, 32};
   double best_ms = 1e300;
-  int best_g = 32;
-  for (int k = 0; k < 3; ++k) {
+  int best_cfg = kTuneCand[2];
+  for (int k = 0; k < kEnsCandidates; ++k) {
     c->ens_accel_valid = true;  // time steps only; the force of the start state is reused
-    PHYS_TRY(ensemble_run(c, p, dt, probe_steps, cand[k], probe_steps));
+    PHYS_TRY(ensemble_run(c, p, dt, probe_steps, kTuneCand[k], probe_steps));
     float ms = 0.f;
     PHYS_CUDA(c, cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]));
-    if (ms3) ms3[k] = ms;
+    if (ms_out) ms_out[k] = ms;
     if (ms < best_ms) {
       best_ms = ms;
-      best_g = cand[k];
+      best_cfg = kTuneCand[k];
     }
     PHYS_CUDA(c, cudaMemcpyAsync(v.x, save, sizeof(double) * 9 * n, cudaMemcpyDeviceToDevice,
                                  c->stream));
   }
   PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
   c->ens_accel_valid = valid0;
-  c->ens_group = best_g;
-  if (best) *best = best_g;
+  c->ens_group = best_cfg;
+  if (best) *best = best_cfg;
   return PHYS_OK;
 }
 

@@ -28,6 +28,17 @@ DIRECT, BARNES_HUT = 0, 1
 F64_EXACT, F64, F32C = 0, 1, 2
 GROUP_WALK = 1  # phys_params.flags: Barnes-Hut walk per group of 64 bodies
 COMP_POSITION, COMP_VELOCITY, COMP_ACCELERATION, COMP_PREV_ACCELERATION, COMP_MASS = range(5)
+# Ensemble launch configurations: lanes per system (8, 16, 32 or ENS_BY_SIZE)
+# | ens_warps(warps per block); the autotuner's candidates, in its order.
+ENS_BY_SIZE = 1
+
+
+def ens_warps(w):
+    return w << 8
+
+
+ENS_CANDIDATES = (8 | 2 << 8, 16 | 2 << 8, 32 | 2 << 8, ENS_BY_SIZE | 2 << 8, 32 | 4 << 8,
+                  ENS_BY_SIZE | 4 << 8)
 
 PRECISIONS = {"f64_exact": F64_EXACT, "f64": F64, "f32c": F32C}
 
@@ -360,12 +371,13 @@ class Context:
         return st(*out[0:3]), st(*out[3:6]), st(*out[6:9])
 
     def ensemble_autotune(self, params, dt, probe_steps=8):
+        """(best configuration code, {code: ms}) over ENS_CANDIDATES."""
         best = ctypes.c_int32()
-        ms = np.zeros(3)
+        ms = np.zeros(len(ENS_CANDIDATES))
         self._check(self.lib.phys_ensemble_autotune(self.h, ctypes.byref(params), float(dt),
                                                     int(probe_steps), ctypes.byref(best), _p(ms)),
                     "phys_ensemble_autotune")
-        return best.value, dict(zip((8, 16, 32), ms.tolist()))
+        return best.value, dict(zip(ENS_CANDIDATES, ms.tolist()))
 
     # ---- trajectory gradients ----
     def adjoint(self, params, dt, nsteps, targets, checkpoint=32):

@@ -29,6 +29,13 @@ pub const PHYS_COMP_ACCELERATION: i32 = 2;
 pub const PHYS_COMP_PREV_ACCELERATION: i32 = 3;
 pub const PHYS_COMP_MASS: i32 = 4;
 
+pub const PHYS_ENS_BY_SIZE: i32 = 1;
+pub const PHYS_ENS_CANDIDATES: i32 = 6;
+/// Warps per block in an ensemble configuration code.
+pub const fn phys_ens_warps(w: i32) -> i32 {
+    w << 8
+}
+
 /// Opaque device context.
 #[repr(C)]
 pub struct phys_ctx {
@@ -143,13 +150,13 @@ extern "C" {
                               x: *const f64, y: *const f64, z: *const f64, vx: *const f64,
                               vy: *const f64, vz: *const f64, m: *const f64) -> c_int;
     pub fn phys_ensemble_run(ctx: *mut phys_ctx, p: *const phys_params, dt: f64, nsteps: i64,
-                             group: i32, chunk: i64) -> c_int;
+                             config: i32, chunk: i64) -> c_int;
     pub fn phys_ensemble_download(ctx: *mut phys_ctx, x: *mut f64, y: *mut f64, z: *mut f64,
                                   vx: *mut f64, vy: *mut f64, vz: *mut f64, ax: *mut f64,
                                   ay: *mut f64, az: *mut f64) -> c_int;
     pub fn phys_ensemble_autotune(ctx: *mut phys_ctx, p: *const phys_params, dt: f64,
-                                  probe_steps: i64, best_group: *mut i32,
-                                  ms3: *mut f64) -> c_int;
+                                  probe_steps: i64, best_config: *mut i32,
+                                  ms: *mut f64) -> c_int;
 
     // ---- trajectory gradients ----
     pub fn phys_adjoint_direct(ctx: *mut phys_ctx, p: *const phys_params, dt: f64, nsteps: i64,

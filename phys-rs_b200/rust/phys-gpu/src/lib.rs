@@ -356,10 +356,23 @@ impl PhysGpu {
         })
     }
 
-    /// nsteps ticks of every system; group 0 autotunes the lanes per system.
-    pub fn ensemble_run(&mut self, p: &ffi::phys_params, dt: f64, nsteps: i64, group: i32,
+    /// nsteps ticks of every system; config 0 uses the autotuned launch shape
+    /// (lanes per system | ffi::phys_ens_warps(warps per block) otherwise).
+    pub fn ensemble_run(&mut self, p: &ffi::phys_params, dt: f64, nsteps: i64, config: i32,
                         chunk: i64) -> Result<()> {
-        self.check(unsafe { ffi::phys_ensemble_run(self.raw(), p, dt, nsteps, group, chunk) })
+        self.check(unsafe { ffi::phys_ensemble_run(self.raw(), p, dt, nsteps, config, chunk) })
+    }
+
+    /// Times every candidate launch shape and keeps the fastest: (best
+    /// configuration code, the candidates' timings in ms).
+    pub fn ensemble_autotune(&mut self, p: &ffi::phys_params, dt: f64, probe_steps: i64)
+                             -> Result<(i32, Vec<f64>)> {
+        let mut best = 0i32;
+        let mut ms = vec![0.0f64; ffi::PHYS_ENS_CANDIDATES as usize];
+        self.check(unsafe {
+            ffi::phys_ensemble_autotune(self.raw(), p, dt, probe_steps, &mut best, ms.as_mut_ptr())
+        })?;
+        Ok((best, ms))
     }
 
     /// Reverse mode: loss and gradient of L = sum_i |x_i(T) - target_i|^2

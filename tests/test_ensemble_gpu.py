@@ -31,7 +31,9 @@ def edge_ensemble():
     return off, pos, vel, m
 
 
-@pytest.mark.parametrize("group", [8, 16, 32])
+@pytest.mark.parametrize("group", [8, 16, 32, physgpu.ENS_BY_SIZE,
+                                   32 | physgpu.ens_warps(4),
+                                   physgpu.ENS_BY_SIZE | physgpu.ens_warps(4)])
 def test_exact_bitexact_vs_oracle(ctx, group):
     off, pos, vel, m = edge_ensemble()
     ctx.ensemble_load(off, pos, vel, m)
@@ -89,7 +91,7 @@ def test_autotune_and_default_group(ctx):
     ctx.ensemble_load(off, pos, vel, m)
     p = make_params(1.0, 1e-3, precision=F32C)
     best, ms = ctx.ensemble_autotune(p, 1e-4, probe_steps=5)
-    assert best in (8, 16, 32) and all(t > 0 for t in ms.values())
+    assert best in physgpu.ENS_CANDIDATES and all(t > 0 for t in ms.values())
     assert ms[best] == min(ms.values())
     x0, v0, _ = ctx.ensemble_download()
     assert np.array_equal(x0[:, 0], pos[:, 0])  # probes leave the state untouched
@@ -103,3 +105,37 @@ def test_oversized_system_rejected(ctx):
     with pytest.raises(physgpu.PhysError) as ei:
         ctx.ensemble_load(off, np.zeros((65, 3)), None, np.ones(65))
     assert ei.value.status == physgpu.ERR_ARG
+
+
+@pytest.mark.parametrize("config", [8, 16, 32, physgpu.ENS_BY_SIZE,
+                                    physgpu.ENS_BY_SIZE | physgpu.ens_warps(4)])
+def test_f32c_every_configuration_close_to_exact(ctx, config):
+    """Every launch shape the autotuner may pick (lanes per system, lanes by
+    size, the split layout of 33-64-body systems on 32 lanes, 2 or 4 warps
+    per block) on systems of every size 1..64."""
+    rng = np.random.default_rng(9)
+    sizes = np.concatenate([np.arange(1, 65), rng.integers(3, 65, 200)])
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    n = int(off[-1])
+    pos = rng.uniform(-1, 1, (n, 3))
+    vel = rng.normal(0, 0.3, (n, 3))
+    m = np.exp(rng.uniform(np.log(0.1), np.log(10), n))
+    ctx.ensemble_load(off, pos, vel, m)
+    ctx.ensemble_run(make_params(1.0, 1e-3, precision=F64_EXACT), 1e-4, 1, group=8)
+    _, _, a64 = ctx.ensemble_download()
+    ctx.ensemble_load(off, pos, vel, m)
+    ctx.ensemble_run(make_params(1.0, 1e-3, precision=F32C), 1e-4, 1, group=config)
+    _, _, a32 = ctx.ensemble_download()
+    nz = np.linalg.norm(a64, axis=1) > 0
+    da = np.linalg.norm(a32 - a64, axis=1)[nz] / np.linalg.norm(a64, axis=1)[nz]
+    assert np.median(da) < 1e-6 and da.max() < 1e-4, (np.median(da), da.max())
+    assert np.all(a32[~nz] == 0)
+
+
+def test_bad_configuration_rejected(ctx):
+    off, pos, vel, m = small_ensemble(10, seed=1)
+    ctx.ensemble_load(off, pos, vel, m)
+    for bad in (7, 64, 32 | physgpu.ens_warps(3), 1 << 20):
+        with pytest.raises(physgpu.PhysError) as ei:
+            ctx.ensemble_run(make_params(1.0, 1e-3, precision=F32C), 1e-4, 1, group=bad)
+        assert ei.value.status == physgpu.ERR_ARG
