@@ -670,11 +670,19 @@ gnode_kernel(int64_t nnodes, const uint32_t* __restrict__ bfs2pre,
   }
 }
 
-// Target groups of the group walk: every cell with more than kGroupMax
+// Bodies per target group that the build aims at (at most kGroupMax, the
+// walk's capacity).
+#ifndef GWALK_GROUP_BODIES
+#define GWALK_GROUP_BODIES 64
+#endif
+constexpr int kGroupBuild = GWALK_GROUP_BODIES;
+static_assert(kGroupBuild >= 1 && kGroupBuild <= kGroupMax, "group size");
+
+// Target groups of the group walk: every cell with more than kGroupBuild
 // bodies splits its children into runs of consecutive children with at most
-// kGroupMax bodies between them (a child with more starts its own groups);
+// kGroupBuild bodies between them (a child with more starts its own groups);
 // a leaf with more (guard depth) is cut into chunks; a root with at most
-// kGroupMax bodies is one group.  The groups partition the bodies into
+// kGroupBuild bodies is one group.  The groups partition the bodies into
 // key-contiguous ranges that each lie inside one cell.  Cells are taken in
 // breadth-first order, so the groups of large shallow cells (the sparse
 // outskirts, whose walks are the longest) come first and the walk's dynamic
@@ -701,20 +709,20 @@ __global__ void group_kernel(int64_t nnodes, const uint32_t* __restrict__ bfs2pr
       if (kEmit && off[j] + r < cap) out[off[j] + r] = make_int2(b0, b1);
       ++r;
     };
-    if (ck <= kGroupMax) {
+    if (ck <= kGroupBuild) {
       if (k == 0) put(lk.y, lk.z);
     } else if (lk.w & kMetaLeaf) {
-      for (int b = lk.y; b < lk.z; b += kGroupMax) put(b, min(b + kGroupMax, lk.z));
+      for (int b = lk.y; b < lk.z; b += kGroupBuild) put(b, min(b + kGroupBuild, lk.z));
     } else {
       int c = (int)k + 1, rb = -1, re = -1;
       const int nc = nchild[k];
       for (int i = 0; i < nc && c < nnodes; ++i) {
         const int4 lc = link[c];
         const int cc = lc.z - lc.y;
-        if (cc > kGroupMax) {
+        if (cc > kGroupBuild) {
           if (rb >= 0) put(rb, re);
           rb = -1;
-        } else if (rb >= 0 && re - rb + cc <= kGroupMax) {
+        } else if (rb >= 0 && re - rb + cc <= kGroupBuild) {
           re = lc.z;
         } else {
           if (rb >= 0) put(rb, re);
