@@ -443,6 +443,16 @@ def run_ours(args, ws, rank, local):
                     "median": float(np.median(e)), "p99": float(np.quantile(e, 0.99)),
                     "max": float(e.max())}
 
+        # ---- the bit-exact reference form (F64_EXACT: the reference's walk,
+        # insertion-order centre of mass, reference op order), leaf capacity 1 ----
+        pex = make_params(1.0, args.eps, args.theta, BARNES_HUT, physgpu.F64_EXACT, 1, 0)
+        ctx.upload(pos, vel, m)
+        ctx.verlet_steps(pex, args.dt, 1)
+        tex, wex, _ = timed_steps(pex, 2)
+        extras["exact_f64_bh_ms_per_step"] = tex / 2
+        extras["exact_f64_bh_walk_ms"] = statistics.median(wex)
+        extras["exact_f64_bh_tree_ms"] = ctx.timings()["tree_ms"]
+
     # ---- roofline of the dominant kernel (the walk) ----
     fp32_tf, fp32x2_tf, fp64_tf = ctx.probe_peaks()
     fp32_peak = max(fp32_tf, fp32x2_tf)

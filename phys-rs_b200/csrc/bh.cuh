@@ -101,7 +101,10 @@ struct BhTree {
 };
 
 // tree.cu
-int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool need_group = false);
+// full_com: the reference-form centre of mass of every cell (export); else
+// cells no target can take as a monopole get only their mass.
+int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool need_group = false,
+             bool full_com = true);
 // walk.cu
 int bh_group_walk(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force,
                   double* ox, double* oy, double* oz);

@@ -38,6 +38,7 @@ struct TreeHeader {
   int32_t dstar;                 // guard depth: first d with d >= 40 or h_d < 1e-8
   int32_t nonfinite;             // any non-finite input coordinate
   int64_t nnodes;                // nodes of the current tree
+  double min_mass;               // smallest body mass
 };
 
 }  // namespace phys

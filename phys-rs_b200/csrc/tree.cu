@@ -54,35 +54,38 @@ __global__ void __launch_bounds__(kBlock)
 bbox_partial_kernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
                     const double* __restrict__ z, const double* __restrict__ m,
                     double* __restrict__ part, int32_t* status) {
-  __shared__ double sh[6][kBlock / 32];
-  double v[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+  __shared__ double sh[7][kBlock / 32];
+  double v[7] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY, INFINITY};
   bool bad = false;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const double a = x[i], b = y[i], cc = z[i];
+    const double a = x[i], b = y[i], cc = z[i], mm = m[i];
+    v[6] = fmin(v[6], mm);
     v[0] = fmin(v[0], a);
     v[1] = fmin(v[1], b);
     v[2] = fmin(v[2], cc);
     v[3] = fmax(v[3], a);
     v[4] = fmax(v[4], b);
     v[5] = fmax(v[5], cc);
-    bad |= !isfinite(a) || !isfinite(b) || !isfinite(cc) || !isfinite(m[i]);
+    bad |= !isfinite(a) || !isfinite(b) || !isfinite(cc) || !isfinite(mm);
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < 3; ++k) v[k] = warp_min(v[k]);
 #pragma unroll
   for (int k = 3; k < 6; ++k) v[k] = warp_max(v[k]);
+  v[6] = warp_min(v[6]);
   if (lane == 0)
-    for (int k = 0; k < 6; ++k) sh[k][warp] = v[k];
+    for (int k = 0; k < 7; ++k) sh[k][warp] = v[k];
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status, kStatNonfinite);
   __syncthreads();
   if (warp == 0) {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      double t = lane < kBlock / 32 ? sh[k][lane] : (k < 3 ? INFINITY : -INFINITY);
-      t = k < 3 ? warp_min(t) : warp_max(t);
-      if (lane == 0) part[blockIdx.x * 6 + k] = t;
+    for (int k = 0; k < 7; ++k) {
+      const bool mn = k < 3 || k == 6;
+      double t = lane < kBlock / 32 ? sh[k][lane] : (mn ? INFINITY : -INFINITY);
+      t = mn ? warp_min(t) : warp_max(t);
+      if (lane == 0) part[blockIdx.x * 7 + k] = t;
     }
   }
 }
@@ -94,17 +97,23 @@ __global__ void bbox_final_kernel(int nparts, const double* __restrict__ part, d
   const int lane = threadIdx.x & 31;
   if (threadIdx.x >= 32) return;
   double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  for (int b = lane; b < nparts; b += 32)
+  double mmin = INFINITY;
+  for (int b = lane; b < nparts; b += 32) {
     for (int k = 0; k < 3; ++k) {
-      mn[k] = fmin(mn[k], part[b * 6 + k]);
-      mx[k] = fmax(mx[k], part[b * 6 + 3 + k]);
+      mn[k] = fmin(mn[k], part[b * 7 + k]);
+      mx[k] = fmax(mx[k], part[b * 7 + 3 + k]);
     }
-  for (int o = 16; o > 0; o >>= 1)
+    mmin = fmin(mmin, part[b * 7 + 6]);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
     for (int k = 0; k < 3; ++k) {
       mn[k] = fmin(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
       mx[k] = fmax(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
     }
+    mmin = fmin(mmin, __shfl_xor_sync(0xffffffffu, mmin, o));
+  }
   if (lane != 0) return;
+  hdr->min_mass = mmin;
   // extent = max - min; max_extent = x.max(y).max(z); half = max_extent*0.55 + 1
   const double ex = xsub(mx[0], mn[0]), ey = xsub(mx[1], mn[1]), ez = xsub(mx[2], mn[2]);
   const double max_extent = fmax(fmax(ex, ey), ez);
@@ -504,17 +513,39 @@ expand_kernel(int64_t total, int64_t nnodes, const int32_t* __restrict__ eoff,
   }
 }
 
+//
+// With skip_unused, a cell that no target can take as a monopole gets only
+// its mass (the same running sum) and a NaN centre of mass: a cell of side s
+// is taken only if s^2 < theta^2 |com - x|^2, and com and x both lie in the
+// root cube of half size H (com as a convex combination of bodies: every
+// mass positive, else nothing is skipped), so |com - x|^2 <= 12 H^2; when
+// s^2 >= theta^2 12 H^2 (with a 1e-6 margin for rounding) the walk opens the
+// cell whatever its centre of mass (a NaN distance opens it too).  This is
+// the root for theta <= 0.577 and every internal cell for theta = 0, and it
+// removes the longest chain of dependent divides (the root's, one per body).
 __global__ void __launch_bounds__(kBlock)
 com_recurrence_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
                       const uint64_t* __restrict__ entries, const double* __restrict__ x,
                       const double* __restrict__ y, const double* __restrict__ z,
                       const double* __restrict__ m, double4* __restrict__ mc,
-                      const int32_t* status) {
+                      const int4* __restrict__ link, const TreeHeader* __restrict__ hdr,
+                      int skip_unused, const int32_t* status) {
   if (sort_failed(status)) return;
+  // the bound holds when every centre of mass is a convex combination of
+  // bodies (all masses positive)
+  const bool can_skip = skip_unused && hdr->min_mass > 0.0;
+  const double bound = hdr->theta2 * 12.0 * hdr->half * hdr->half * (1.0 + 1e-6);
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnodes;
        k += (int64_t)gridDim.x * blockDim.x) {
     const int64_t e0 = eoff[k], e1 = eoff[k + 1];
     double M = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
+    if (can_skip && !(link[k].w & kMetaLeaf) && hdr->s2[link[k].w & kMetaDepth] >= bound) {
+      for (int64_t e = e0; e < e1; ++e) M = xadd(M, m[(uint32_t)(entries[e] & 0xffffffffu)]);
+      mc[k] = make_double4(__longlong_as_double(0x7ff8000000000000ll),
+                           __longlong_as_double(0x7ff8000000000000ll),
+                           __longlong_as_double(0x7ff8000000000000ll), M);
+      continue;
+    }
     constexpr int kB = 8;
     for (int64_t e = e0; e < e1; e += kB) {
       double bx[kB], by[kB], bz[kB], bm[kB];
@@ -741,7 +772,8 @@ __global__ void group_kernel(int64_t nnodes, const uint32_t* __restrict__ bfs2pr
 
 // Builds the tree for the current positions.  One host synchronisation reads
 // the node count (two with bucket leaves).
-int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool need_group) {
+int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool need_group,
+             bool full_com) {
   const int64_t n = c->n;
   const bool exact = p->precision == PHYS_F64_EXACT;
   uint64_t* khi = nullptr;
@@ -772,7 +804,7 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
   PHYS_TRY(ws_alloc(c, WS_NCOUNT, n + 1, &cnt));
   int32_t* first = nullptr;
   PHYS_TRY(ws_alloc(c, WS_NFIRST, n + 1, &first));
-  if (!c->d_partials || c->partials_cap < 6 * kBboxGrid) {
+  if (!c->d_partials || c->partials_cap < 7 * kBboxGrid) {
     if (c->d_partials) cudaFree(c->d_partials);
     c->d_partials = nullptr;
     PHYS_CUDA(c, cudaMalloc(&c->d_partials, sizeof(double) * 8 * kBboxGrid));
@@ -877,7 +909,7 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
     PHYS_TRY(radix_sort_u64(c, e1, nullptr, e1_alt, nullptr, total, 32, 32 + bits_n, &alt2));
     uint64_t* es = alt2 ? e1_alt : e1;
     PHYS_LAUNCH(c, com_recurrence_kernel, grid_for(nnodes, 128, 1 << 30), 128, 0, nnodes, eoff, es,
-                c->x, c->y, c->z, c->m, mc, c->d_status);
+                c->x, c->y, c->z, c->m, mc, link, c->d_hdr, full_com ? 0 : 1, c->d_status);
   } else {
     PHYS_CUDA(c, cudaMemsetAsync(arrive, 0, sizeof(int32_t) * (nnodes + 1), c->stream));
     PHYS_LAUNCH(c, com_upward_kernel, grid_for(nnodes), kBlock, 0, nnodes, link, parent, nchild,
@@ -961,7 +993,9 @@ int bh_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, doub
             double* oz) {
   BhTree t;
   const bool group = (p->flags & PHYS_FLAG_GROUP_WALK) != 0;
-  PHYS_TRY(bh_build(c, p, p->precision == PHYS_F32C && !group, &t, group));
+  // the exact form's forces need no centre of mass of cells no target can
+  // take as a monopole
+  PHYS_TRY(bh_build(c, p, p->precision == PHYS_F32C && !group, &t, group, false));
   return bh_walk(c, p, t, want_force, ox, oy, oz);
 }
 
