@@ -90,8 +90,8 @@ struct phys_ctx {
   // context, after the context has made its own device current; nothing is
   // shared between contexts or threads.  occ_gwalk: resident blocks per SM of
   // the group-walk kernels (list, evaluation F64 / F32C, re-queued walk F64 /
-  // F32C, list + evaluation F64 / F32C), 0 until queried.
-  int occ_gwalk[7] = {};
+  // F32C), 0 until queried.
+  int occ_gwalk[5] = {};
   bool sort_smem_set = false;
   // Bound on one look-back wait of the radix sort, in re-reads of a tile's
   // status word (see sort.cu); phys_debug_set_wait_limit lowers it in tests.

@@ -76,8 +76,8 @@
 #ifndef GEVAL_MIN_BLOCKS
 #define GEVAL_MIN_BLOCKS 4
 #endif
-#ifndef GWALK_FUSED
-#define GWALK_FUSED 1
+#ifndef GWALK_PREFETCH
+#define GWALK_PREFETCH 0
 #endif
 #ifndef GWALK_POOL_PER_BODY
 #define GWALK_POOL_PER_BODY 128
@@ -310,6 +310,15 @@ __device__ __forceinline__ int traverse(int lane, int base, int gend, int nnodes
     const int etot = __shfl_sync(kFull, ein, 31);
     if (__any_sync(kFull, o.malformed) || ssize + ptot > kGStack) return -1;
     for (int c = 0; c < o.npush; ++c) stk[ssize + pin - o.npush + c] = o.cfirst + c;
+    if (GWALK_PREFETCH && o.npush > 0) {
+      // the children are popped in the next rounds: bring their records
+      // (contiguous, breadth-first) into L1 now, so those rounds' loads do
+      // not wait for L2
+      const uintptr_t a0 = reinterpret_cast<uintptr_t>(gn + o.cfirst) & ~uintptr_t(127);
+      const uintptr_t a1 = reinterpret_cast<uintptr_t>(gn + o.cfirst + o.npush);
+      for (uintptr_t a = a0; a < a1; a += 128)
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(a));
+    }
     ssize += ptot;
     listed += etot;
     if (etot > 0 && !sink(etot, ein - o.nent, o)) return 0;
@@ -712,7 +721,7 @@ struct Evaluator {
 #pragma unroll
       for (int j = 0; j < kPer; ++j) {
         const int e = b * kL + lane + 32 * j;
-        pc[j] = e < len ? __ldcg(codes + e) : ~0u;  // L2: may be this kernel's writes
+        pc[j] = e < len ? __ldcg(codes + e) : ~0u;  // read once: L2 only
       }
     };
     auto issue = [&](int b) {
@@ -993,94 +1002,6 @@ geval_kernel(int n, const GNode* __restrict__ gn, const int4* __restrict__ items
 }
 
 // ---------------------------------------------------------------------------
-// 2'. list building and evaluation in one kernel: each warp walks a group,
-// writes its list to the warp's own pool region (a few tens of KB, which
-// stays in L2) and streams it through the evaluator at once; the walk's
-// stack and the evaluator's buffers share the warp's shared memory.  While
-// some warps wait on tree reads in their walks, the others keep the FP32
-// pipe busy, so the latency-bound list building overlaps the evaluation.
-// ---------------------------------------------------------------------------
-constexpr int kFSmemWarp = kESmemWarp > kGStack * 4 ? kESmemWarp : kGStack * 4;
-constexpr int kFSmem = kGWarps * kFSmemWarp;
-
-template <bool kF32>
-__global__ void __launch_bounds__(kGBlock, GEVAL_MIN_BLOCKS)
-gfused_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __restrict__ groups,
-              const int32_t* __restrict__ ngroups_p, int32_t* __restrict__ ctr,
-              const double4* __restrict__ body64, const uint32_t* __restrict__ perm, double G,
-              double eps2, float theta2f, int want_force, double* __restrict__ ox,
-              double* __restrict__ oy, double* __restrict__ oz, uint32_t* __restrict__ pool,
-              int64_t pool_per_warp, int2* __restrict__ retry, int32_t* __restrict__ nretry,
-              unsigned long long* counter, int32_t* status) {
-  if (sort_failed(status)) return;  // records built on an unfinished sort
-  extern __shared__ __align__(16) unsigned char gsm[];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  unsigned char* ws = gsm + wid * kFSmemWarp;
-  int* stk = reinterpret_cast<int*>(ws);  // walk phase; the evaluator's buffers after it
-  uint32_t* region = pool + (blockIdx.x * (int64_t)kGWarps + wid) * pool_per_warp;
-  const int cap = (int)min64(pool_per_warp, (int64_t)INT_MAX);
-  const int ngroups = min(*ngroups_p, n);
-  unsigned long long ninter = 0;
-  bool bad = false;
-  for (;;) {
-    const int gi = next_item(lane, ctr);
-    if (gi >= ngroups) break;
-    const int2 gr = groups[gi];
-    if (bad_range(gr, n)) {
-      bad = true;
-      break;
-    }
-    const int base = gr.x, gend = gr.y;
-    const double4 X0 = body64[base];
-    const int ia = base + 2 * lane, ib = ia + 1;
-    const double4 ta = ia < gend ? body64[ia] : X0;
-    const double4 tb = ib < gend ? body64[ib] : X0;
-    const Box B = group_box(X0, ta, tb);
-    int used = 0;
-    auto sink = [&](int etot, int eoff, const NodeOut& o) -> bool {
-      if (used + etot > cap) return false;  // region full: re-queue
-      uint32_t* dst = region + used + eoff;
-      if (o.kind == 1) {
-        dst[0] = (uint32_t)o.a << 1;
-      } else {
-        for (int j = 0; j < o.nent; ++j)
-          dst[j] = ((uint32_t)bucket_body(o.a, o.olo, o.ohi, j) << 1) | 1u;
-      }
-      used += etot;
-      return true;
-    };
-    const int r = traverse<false>(lane, base, gend, nnodes, kGListLimit, stk, B, theta2f, gn,
-                                  sink);
-    if (r < 0) {
-      bad = true;
-      break;
-    }
-    if (r == 0) {
-      if (lane == 0 && !requeue(gr, n, retry, nretry)) bad = true;
-      __syncwarp();
-      continue;
-    }
-    __syncwarp();  // the list is written and the stack is free
-    Evaluator<kF32, kEB> E;
-    E.init(lane, base, gend, body64, ws, eps2);
-    const float far2 =
-        (float)(GWALK_FAR * GWALK_FAR) * fmaf(B.bx, B.bx, fmaf(B.by, B.by, B.bz * B.bz));
-    E.self_pass();
-    ninter += (unsigned long long)E.nvalid * (unsigned long long)(E.nvalid - 1 + used);
-    E.stream_eval(region, used, gn, body64, B, far2, reinterpret_cast<double4*>(ws + kEListBytes));
-    E.finish(body64, perm, G, want_force, ox, oy, oz, status);
-    __syncwarp();  // evaluator buffers read: the next walk may reuse them
-  }
-  if (lane == 0) {
-    if (bad) atomicOr(status, kStatOverflow);
-    if (ninter) {  // the same on every lane
-      atomicAdd(counter, ninter);
-      atomicAdd(counter + 1, ninter);
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
 // 3. walk + evaluation in one pass (re-queued subgroups)
 // ---------------------------------------------------------------------------
 template <bool kF32>
@@ -1207,46 +1128,9 @@ int occupancy(phys_ctx* c, K kernel, int block, int smem, int* cache) {
   return PHYS_OK;
 }
 
-// List building and evaluation fused in one kernel (gfused_kernel), the
-// re-queued single bodies after it; the retry walks need the fused kernel's
-// requeue list, so they run after it on the same stream.
-template <bool kF32>
-int launch_fused(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force,
-                 double* ox, double* oy, double* oz) {
-  int& occ_f = c->occ_gwalk[kF32 ? 6 : 5];
-  int& occ_fused = c->occ_gwalk[kF32 ? 4 : 3];
-  PHYS_TRY(occupancy(c, gfused_kernel<kF32>, kGBlock, kFSmem, &occ_f));
-  PHYS_TRY(occupancy(c, gwalk_kernel<kF32>, kGBlock, kGSmem, &occ_fused));
-  int sms = 0;
-  PHYS_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-  const int64_t n = t.n;
-  const int grid = (int)min64((int64_t)sms * occ_f, ceil_div(n, (int64_t)kGWarps));
-  const int grid_retry = (int)min64((int64_t)sms * occ_fused, ceil_div(n, (int64_t)kGWarps));
-  // one list at a time per warp: the first-pass budget plus one round's entries
-  const int64_t pool_per_warp = (int64_t)kGListLimit + 32 * 8 + 64;
-  uint32_t* pool = nullptr;
-  PHYS_TRY(ws_alloc(c, WS_GROUP_POOL, (int64_t)grid * kGWarps * pool_per_warp, &pool));
-  // group_ctr: [0] group counter, [1] re-queued count, [4] retry-walk counter
-  int32_t* ctr = t.group_ctr;
-  PHYS_CUDA(c, cudaMemsetAsync(ctr, 0, 5 * sizeof(int32_t), c->stream));
-  const double eps2 = p->eps * p->eps;
-  const float theta2f = (float)(p->theta * p->theta);
-  int2* retry = const_cast<int2*>(t.groups) + n;
-  PHYS_CUDA(c, cudaEventRecord(c->ev[10], c->stream));
-  PHYS_LAUNCH(c, gfused_kernel<kF32>, grid, kGBlock, kFSmem, (int)n, (int)t.nnodes, t.gnode,
-              t.groups, t.ngroups, ctr, t.body64, t.perm, p->G, eps2, theta2f, (int)want_force,
-              ox, oy, oz, pool, pool_per_warp, retry, ctr + 1, c->d_counter, c->d_status);
-  PHYS_CUDA(c, cudaEventRecord(c->ev[11], c->stream));
-  PHYS_LAUNCH(c, gwalk_kernel<kF32>, grid_retry, kGBlock, kGSmem, (int)n, (int)t.nnodes, t.gnode,
-              retry, ctr + 1, ctr + 4, t.body64, t.perm, p->G, eps2, theta2f, (int)want_force, ox,
-              oy, oz, c->d_counter, c->d_status);
-  return PHYS_OK;
-}
-
 template <bool kF32>
 int launch(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force, double* ox,
            double* oy, double* oz) {
-  if (GWALK_FUSED) return launch_fused<kF32>(c, p, t, want_force, ox, oy, oz);
   int& occ_list = c->occ_gwalk[0];
   int& occ_eval = c->occ_gwalk[kF32 ? 2 : 1];
   int& occ_fused = c->occ_gwalk[kF32 ? 4 : 3];
