@@ -56,7 +56,7 @@
 #include "bh.cuh"
 
 #ifndef GWALK_FLUSH_PAIRS
-#define GWALK_FLUSH_PAIRS 32
+#define GWALK_FLUSH_PAIRS 64
 #endif
 #ifndef GWALK_LIST_LIMIT
 #define GWALK_LIST_LIMIT 8192
@@ -65,7 +65,7 @@
 #define GWALK_SPLIT 1
 #endif
 #ifndef GWALK_FAR
-#define GWALK_FAR 0.25
+#define GWALK_FAR 0.0625
 #endif
 #ifndef GEVAL_UNROLL
 #define GEVAL_UNROLL 2
@@ -107,11 +107,15 @@ constexpr int kGSmem = kGWarps * kGSmemWarp;
 constexpr int kLSmem = kLWarps * kGStack * 4;  // list kernel: stacks
 // evaluation kernel, per warp: near list (7 arrays) | far list (4 arrays) of
 // kEB entries, then two staging buffers of kEB source records
-constexpr int kEB = 128;
+#ifndef GEVAL_BATCH
+#define GEVAL_BATCH 128
+#endif
+constexpr int kEB = GEVAL_BATCH;  // list entries per staging batch
 constexpr int kEListBytes = kEB * 7 * 4 + kEB * 4 * 4;
 constexpr int kESmemWarp = kEListBytes + 2 * kEB * 32;
 constexpr int kESmem = kGWarps * kESmemWarp;
-static_assert(kEListBytes % 32 == 0 && kEB >= kGroupMax, "evaluation kernel layout");
+static_assert(kEListBytes % 32 == 0 && kEB >= kGroupMax && kEB % 32 == 0,
+              "evaluation kernel layout");
 static_assert(kGroupMax == 64, "two targets per lane");
 static_assert(kGThrottle >= 7 * 32 + 7, "stack too small for batched pops");
 static_assert(kGThrottle + 7 * kMaxLevels + 1 <= kGStack, "stack bound");
@@ -705,10 +709,10 @@ struct Evaluator {
   // distance from the group's box is at least GWALK_FAR box half-diagonals b
   // goes to the far list, whose plain f32 offsets from X0 need no low parts
   // (targets lie within 2b of X0, so the separation's error is below
-  // 2^-24 (2|r| + 4b) <= 18 * 2^-24 |r| at a quarter half-diagonal, a few
-  // times the f32 pair term's own rounding); the rest go to the near list
-  // (double-float).  F64: the staged
-  // records are the list.
+  // 2^-24 (2|r| + 4b) <= 66 * 2^-24 |r| at a sixteenth of a half-diagonal,
+  // about 4e-6 for the nearest far entries and far less for most: the
+  // F32C-vs-F64 median stays at 5e-8); the rest go to the near list
+  // (double-float).  F64: the staged records are the list.
   __device__ __forceinline__ void stream_eval(const uint32_t* __restrict__ codes, int len,
                                               const GNode* __restrict__ gn,
                                               const double4* __restrict__ body64, const Box& B,
