@@ -11,6 +11,7 @@
 // The host captures the chunk launches of a run in a CUDA graph; an
 // autotuner picks G by timing a few steps of each candidate.
 #include <algorithm>
+#include <cstddef>
 #include <numeric>
 #include <vector>
 
@@ -38,6 +39,11 @@ struct GroupSmemT {
 using GroupSmem = GroupSmemT<kMaxSys>;
 // With lanes per system chosen by size, a warp's shared memory holds one
 // 64-body group, two 16-body groups or four 8-body groups in turn.
+// quads of sources are read with 16-byte loads
+static_assert(sizeof(GroupSmemT<8>) % 16 == 0 && sizeof(GroupSmemT<16>) % 16 == 0 &&
+                  sizeof(GroupSmem) % 16 == 0 && offsetof(GroupSmemT<8>, hx) % 16 == 0 &&
+                  offsetof(GroupSmemT<8>, hy) % 16 == 0,
+              "16-byte aligned source arrays");
 static_assert(2 * sizeof(GroupSmemT<16>) <= sizeof(GroupSmem) &&
                   4 * sizeof(GroupSmemT<8>) <= sizeof(GroupSmem),
               "sub-warp groups fit in a warp's share");
@@ -66,32 +72,40 @@ __device__ __forceinline__ void set_pad(S_t* S, int i) {
   S->hm[i] = S->lx[i] = S->ly[i] = S->lz[i] = 0.f;
 }
 
-__device__ __forceinline__ float2 ld2(const float* p) {
-  return *reinterpret_cast<const float2*>(p);
-}
+__device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
 
-// One source pair (bodies j, j + 1) against one target; skip0 / skip1 zero
-// the half that is the target itself (i == j is skipped, gravity.rs:56).
-struct PairSrc {
-  float2 sx, sy, sz, sm, tx, ty, tz;
+// Four consecutive sources (bodies j..j+3, j a multiple of 4) in seven
+// 16-byte shared-memory loads; slots past N are massless pads far away.
+struct QuadSrc {
+  float4 sx, sy, sz, sm, tx, ty, tz;
 };
 template <class S_t>
-__device__ __forceinline__ PairSrc load_pair(const S_t* S, int j) {
-  return PairSrc{ld2(S->hx + j), ld2(S->hy + j), ld2(S->hz + j), ld2(S->hm + j),
-                 ld2(S->lx + j), ld2(S->ly + j), ld2(S->lz + j)};
+__device__ __forceinline__ QuadSrc load_quad(const S_t* S, int j) {
+  auto q = [&](const float* a) { return *reinterpret_cast<const float4*>(a + j); };
+  return QuadSrc{q(S->hx), q(S->hy), q(S->hz), q(S->hm), q(S->lx), q(S->ly), q(S->lz)};
 }
-__device__ __forceinline__ void pair_term(const PairSrc& s, float2 nhx, float2 nhy, float2 nhz,
-                                          float2 nlx, float2 nly, float2 nlz, float2 e2,
-                                          bool skip0, bool skip1, float2& px, float2& py,
-                                          float2& pz) {
-  const float2 rx = __fadd2_rn(__fadd2_rn(s.sx, nhx), __fadd2_rn(s.tx, nlx));
-  const float2 ry = __fadd2_rn(__fadd2_rn(s.sy, nhy), __fadd2_rn(s.ty, nly));
-  const float2 rz = __fadd2_rn(__fadd2_rn(s.sz, nhz), __fadd2_rn(s.tz, nlz));
+
+// One source pair against one target.  kSkip zeroes the halves that are
+// the target itself (i == j is skipped, gravity.rs:56); with eps^2 > 0 it is
+// not needed: the self separation is exactly 0 (hi - hi + lo - lo) and
+// r^2 = eps^2, so the term adds exactly 0.
+template <bool kSkip>
+__device__ __forceinline__ void pair_term(float2 sx, float2 sy, float2 sz, float2 sm, float2 tx,
+                                          float2 ty, float2 tz, float2 nhx, float2 nhy,
+                                          float2 nhz, float2 nlx, float2 nly, float2 nlz,
+                                          float2 e2, bool skip0, bool skip1, float2& px,
+                                          float2& py, float2& pz) {
+  const float2 rx = __fadd2_rn(__fadd2_rn(sx, nhx), __fadd2_rn(tx, nlx));
+  const float2 ry = __fadd2_rn(__fadd2_rn(sy, nhy), __fadd2_rn(ty, nly));
+  const float2 rz = __fadd2_rn(__fadd2_rn(sz, nhz), __fadd2_rn(tz, nlz));
   const float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __ffma2_rn(rz, rz, e2)));
   const float2 inv = make_float2(rsqrt_sfu(r2.x), rsqrt_sfu(r2.y));
-  float2 w = __fmul2_rn(s.sm, __fmul2_rn(__fmul2_rn(inv, inv), inv));
-  if (skip0) w.x = 0.f;
-  if (skip1) w.y = 0.f;
+  float2 w = __fmul2_rn(sm, __fmul2_rn(__fmul2_rn(inv, inv), inv));
+  if (kSkip) {
+    if (skip0) w.x = 0.f;
+    if (skip1) w.y = 0.f;
+  }
   px = __ffma2_rn(rx, w, px);
   py = __ffma2_rn(ry, w, py);
   pz = __ffma2_rn(rz, w, pz);
@@ -106,44 +120,63 @@ __device__ __forceinline__ void fold(float2& p, float& h, float& l) {
   p = make_float2(0.f, 0.f);
 }
 
-// F32C accelerations of the group's own targets, TC targets per pass.  Two
-// sources per packed f32x2 operation (bodies j, j+1; an odd N reads the pad
-// at slot N); partial sums of 16 sources folded into a (hi, lo) accumulator
-// by two-sum.
-template <int G, int TC, class S_t>
+// The negated double-float position of target i, packed for f32x2 terms.
+struct TargetNeg {
+  float2 hx, hy, hz, lx, ly, lz;
+};
+template <class S_t>
+__device__ __forceinline__ TargetNeg target_neg(const S_t* S, int i) {
+  auto n = [](float v) { return make_float2(-v, -v); };
+  return TargetNeg{n(S->hx[i]), n(S->hy[i]), n(S->hz[i]), n(S->lx[i]), n(S->ly[i]), n(S->lz[i])};
+}
+
+// F32C accelerations of the group's own targets, TC targets per pass.  The
+// sources come four at a time (two packed f32x2 pairs: sources j, j+1 and
+// j+2, j+3); with one target per lane the two pairs go to separate partial
+// sums, so two dependency chains interleave.  Partial sums of 16 sources are
+// folded into a (hi, lo) accumulator by two-sum.
+template <int G, int TC, bool kSkip, class S_t>
 __device__ void group_forces_f32c(S_t* S, int N, int gl, double Gc, float eps2f) {
   const float2 e2 = make_float2(eps2f, eps2f);
+  constexpr int kSets = TC == 1 ? 2 : 1;
+  const int n4 = (N + 3) & ~3;
   for (int i0 = gl; i0 < N; i0 += G * TC) {
-    float2 nhx[TC], nhy[TC], nhz[TC], nlx[TC], nly[TC], nlz[TC], px[TC], py[TC], pz[TC];
+    TargetNeg tn[TC];
+    float2 px[kSets][TC], py[kSets][TC], pz[kSets][TC];
     float hx[TC], hy[TC], hz[TC], lx[TC], ly[TC], lz[TC];
     int idx[TC];
 #pragma unroll
     for (int t = 0; t < TC; ++t) {
       idx[t] = i0 + t * G;
-      const int ii = idx[t] < N ? idx[t] : i0;
-      nhx[t] = make_float2(-S->hx[ii], -S->hx[ii]);
-      nhy[t] = make_float2(-S->hy[ii], -S->hy[ii]);
-      nhz[t] = make_float2(-S->hz[ii], -S->hz[ii]);
-      nlx[t] = make_float2(-S->lx[ii], -S->lx[ii]);
-      nly[t] = make_float2(-S->ly[ii], -S->ly[ii]);
-      nlz[t] = make_float2(-S->lz[ii], -S->lz[ii]);
+      tn[t] = target_neg(S, idx[t] < N ? idx[t] : i0);
       hx[t] = hy[t] = hz[t] = lx[t] = ly[t] = lz[t] = 0.f;
-      px[t] = py[t] = pz[t] = make_float2(0.f, 0.f);
-    }
-    for (int j0 = 0; j0 < N; j0 += 16) {
-      const int j1 = min(N, j0 + 16);
-      for (int j = j0; j < j1; j += 2) {
-        const PairSrc s = load_pair(S, j);
 #pragma unroll
-        for (int t = 0; t < TC; ++t)
-          pair_term(s, nhx[t], nhy[t], nhz[t], nlx[t], nly[t], nlz[t], e2, j == idx[t],
-                    j + 1 == idx[t], px[t], py[t], pz[t]);
+      for (int k = 0; k < kSets; ++k) px[k][t] = py[k][t] = pz[k][t] = make_float2(0.f, 0.f);
+    }
+    for (int j0 = 0; j0 < n4; j0 += 16) {
+      const int j1 = min(n4, j0 + 16);
+      for (int j = j0; j < j1; j += 4) {
+        const QuadSrc q = load_quad(S, j);
+#pragma unroll
+        for (int t = 0; t < TC; ++t) {
+          const TargetNeg& a = tn[t];
+          pair_term<kSkip>(lo2(q.sx), lo2(q.sy), lo2(q.sz), lo2(q.sm), lo2(q.tx), lo2(q.ty),
+                           lo2(q.tz), a.hx, a.hy, a.hz, a.lx, a.ly, a.lz, e2, j == idx[t],
+                           j + 1 == idx[t], px[0][t], py[0][t], pz[0][t]);
+          pair_term<kSkip>(hi2(q.sx), hi2(q.sy), hi2(q.sz), hi2(q.sm), hi2(q.tx), hi2(q.ty),
+                           hi2(q.tz), a.hx, a.hy, a.hz, a.lx, a.ly, a.lz, e2, j + 2 == idx[t],
+                           j + 3 == idx[t], px[kSets - 1][t], py[kSets - 1][t],
+                           pz[kSets - 1][t]);
+        }
       }
 #pragma unroll
       for (int t = 0; t < TC; ++t) {
-        fold(px[t], hx[t], lx[t]);
-        fold(py[t], hy[t], ly[t]);
-        fold(pz[t], hz[t], lz[t]);
+#pragma unroll
+        for (int k = 0; k < kSets; ++k) {
+          fold(px[k][t], hx[t], lx[t]);
+          fold(py[k][t], hy[t], ly[t]);
+          fold(pz[k][t], hz[t], lz[t]);
+        }
       }
     }
 #pragma unroll
@@ -164,13 +197,14 @@ __device__ __forceinline__ int next_pow2(int v) {
 }
 
 // F32C forces of a 33..64-body system on one warp without idle second
-// slots: lane l takes target a = l over every source pair, and one of the
+// slots: lane l takes target a = l over every source, and one of the
 // nb = N - 32 second targets, b = 32 + l mod lps (lps = nb rounded up to a
-// power of two), over its stream's share of the source pairs: the warp's
-// r = 32 / lps streams take alternate pairs, and their sums for the same b
-// are added by shuffles at the end.  Each round covers r source pairs: all r
-// against a, one (the stream's own) against b.
-template <class S_t>
+// power of two), over its stream's share of the sources: the warp's
+// r = 32 / lps streams take alternate groups of four sources, and their sums
+// for the same b are added by shuffles at the end.  Each round covers r
+// source quads: all r against a (two interleaved chains), one (the
+// stream's own) against b.
+template <bool kSkip, class S_t>
 __device__ void group_forces_f32c_split(S_t* S, int N, int gl, double Gc, float eps2f) {
   const float2 e2 = make_float2(eps2f, eps2f);
   const int nb = N - 32;
@@ -178,34 +212,45 @@ __device__ void group_forces_f32c_split(S_t* S, int N, int gl, double Gc, float 
   const int st = gl / lps, tb = 32 + gl % lps;
   const int ta = gl;
   const int tbv = tb < N ? tb : ta;  // lanes without a valid b compute a dummy (discarded)
-  auto neg = [](float v) { return make_float2(-v, -v); };
-  const float2 ahx = neg(S->hx[ta]), ahy = neg(S->hy[ta]), ahz = neg(S->hz[ta]);
-  const float2 alx = neg(S->lx[ta]), aly = neg(S->ly[ta]), alz = neg(S->lz[ta]);
-  const float2 bhx = neg(S->hx[tbv]), bhy = neg(S->hy[tbv]), bhz = neg(S->hz[tbv]);
-  const float2 blx = neg(S->lx[tbv]), bly = neg(S->ly[tbv]), blz = neg(S->lz[tbv]);
-  float2 pax = make_float2(0.f, 0.f), pay = pax, paz = pax, pbx = pax, pby = pax, pbz = pax;
+  const TargetNeg A = target_neg(S, ta), B = target_neg(S, tbv);
+  const float2 z2 = make_float2(0.f, 0.f);
+  float2 pax0 = z2, pay0 = z2, paz0 = z2, pax1 = z2, pay1 = z2, paz1 = z2;
+  float2 pbx = z2, pby = z2, pbz = z2;
   float hax = 0.f, hay = 0.f, haz = 0.f, lax = 0.f, lay = 0.f, laz = 0.f;
   float hbx = 0.f, hby = 0.f, hbz = 0.f, lbx = 0.f, lby = 0.f, lbz = 0.f;
-  const int npairs = (N + 1) >> 1;
-  int fa = 0, fb = 0;  // pairs in the partial sums
-  for (int q = 0; q < npairs; q += r) {
-    for (int k = 0; k < r && q + k < npairs; ++k) {
-      const int j = 2 * (q + k);
-      pair_term(load_pair(S, j), ahx, ahy, ahz, alx, aly, alz, e2, j == ta, j + 1 == ta, pax,
-                pay, paz);
-      if (++fa == 8) {
-        fold(pax, hax, lax);
-        fold(pay, hay, lay);
-        fold(paz, haz, laz);
+  const int nq = (N + 3) >> 2;  // source quads
+  int fa = 0, fb = 0;           // quads in the partial sums
+  for (int q0 = 0; q0 < nq; q0 += r) {
+    for (int k = 0; k < r && q0 + k < nq; ++k) {
+      const int j = 4 * (q0 + k);
+      const QuadSrc q = load_quad(S, j);
+      pair_term<kSkip>(lo2(q.sx), lo2(q.sy), lo2(q.sz), lo2(q.sm), lo2(q.tx), lo2(q.ty),
+                       lo2(q.tz), A.hx, A.hy, A.hz, A.lx, A.ly, A.lz, e2, j == ta, j + 1 == ta,
+                       pax0, pay0, paz0);
+      pair_term<kSkip>(hi2(q.sx), hi2(q.sy), hi2(q.sz), hi2(q.sm), hi2(q.tx), hi2(q.ty),
+                       hi2(q.tz), A.hx, A.hy, A.hz, A.lx, A.ly, A.lz, e2, j + 2 == ta,
+                       j + 3 == ta, pax1, pay1, paz1);
+      if (++fa == 4) {
+        fold(pax0, hax, lax);
+        fold(pay0, hay, lay);
+        fold(paz0, haz, laz);
+        fold(pax1, hax, lax);
+        fold(pay1, hay, lay);
+        fold(paz1, haz, laz);
         fa = 0;
       }
     }
-    const int pb = q + st;
-    if (pb < npairs) {
-      const int j = 2 * pb;
-      pair_term(load_pair(S, j), bhx, bhy, bhz, blx, bly, blz, e2, j == tbv, j + 1 == tbv, pbx,
-                pby, pbz);
-      if (++fb == 8) {
+    const int qb = q0 + st;
+    if (qb < nq) {
+      const int j = 4 * qb;
+      const QuadSrc q = load_quad(S, j);
+      pair_term<kSkip>(lo2(q.sx), lo2(q.sy), lo2(q.sz), lo2(q.sm), lo2(q.tx), lo2(q.ty),
+                       lo2(q.tz), B.hx, B.hy, B.hz, B.lx, B.ly, B.lz, e2, j == tbv,
+                       j + 1 == tbv, pbx, pby, pbz);
+      pair_term<kSkip>(hi2(q.sx), hi2(q.sy), hi2(q.sz), hi2(q.sm), hi2(q.tx), hi2(q.ty),
+                       hi2(q.tz), B.hx, B.hy, B.hz, B.lx, B.ly, B.lz, e2, j + 2 == tbv,
+                       j + 3 == tbv, pbx, pby, pbz);
+      if (++fb == 4) {
         fold(pbx, hbx, lbx);
         fold(pby, hby, lby);
         fold(pbz, hbz, lbz);
@@ -213,9 +258,12 @@ __device__ void group_forces_f32c_split(S_t* S, int N, int gl, double Gc, float 
       }
     }
   }
-  fold(pax, hax, lax);
-  fold(pay, hay, lay);
-  fold(paz, haz, laz);
+  fold(pax0, hax, lax);
+  fold(pay0, hay, lay);
+  fold(paz0, haz, laz);
+  fold(pax1, hax, lax);
+  fold(pay1, hay, lay);
+  fold(paz1, haz, laz);
   fold(pbx, hbx, lbx);
   fold(pby, hby, lby);
   fold(pbz, hbz, lbz);
@@ -236,8 +284,24 @@ __device__ void group_forces_f32c_split(S_t* S, int N, int gl, double Gc, float 
   }
 }
 
+// Targets per lane for this system: one, or passes of kMaxTC (two) when
+// the system has more bodies than the group has lanes (8 or 16 lanes only:
+// 32 lanes take 33..64 bodies in the split layout).
+template <int G, int kMaxTC, bool kSkip, class S_t>
+__device__ __forceinline__ void group_forces_f32c_any(S_t* S, int N, int gl, double Gc,
+                                                      float eps2f) {
+  if (G == 32 && N > 32) {
+    group_forces_f32c_split<kSkip>(S, N, gl, Gc, eps2f);
+    return;
+  }
+  if (kMaxTC == 1 || N <= G)
+    group_forces_f32c<G, 1, kSkip>(S, N, gl, Gc, eps2f);
+  else
+    group_forces_f32c<G, (kMaxTC > 1 ? 2 : 1), kSkip>(S, N, gl, Gc, eps2f);
+}
+
 // Accelerations of the group's own targets (i = gl, gl+G, ...) into S->a.
-template <int G, bool kExact, class S_t>
+template <int G, bool kExact, int kMaxTC, class S_t>
 __device__ void group_forces(S_t* S, int N, int gl, double Gc, double eps2) {
   if (kExact) {
     for (int i = gl; i < N; i += G) {
@@ -260,18 +324,10 @@ __device__ void group_forces(S_t* S, int N, int gl, double Gc, double eps2) {
     return;
   }
   const float eps2f = (float)eps2;
-  if (G == 32 && N > 32) {
-    group_forces_f32c_split(S, N, gl, Gc, eps2f);
-    return;
-  }
-  // targets per lane for this system: 1, 2 or (up to 8 in passes of) 4
-  const int tpl = (N + G - 1) / G;
-  if (tpl <= 1)
-    group_forces_f32c<G, 1>(S, N, gl, Gc, eps2f);
-  else if (tpl == 2)
-    group_forces_f32c<G, 2>(S, N, gl, Gc, eps2f);
-  else
-    group_forces_f32c<G, 4>(S, N, gl, Gc, eps2f);
+  if (eps2f > 0.f)
+    group_forces_f32c_any<G, kMaxTC, false>(S, N, gl, Gc, eps2f);
+  else  // eps = 0: the self pair must be skipped by index
+    group_forces_f32c_any<G, kMaxTC, true>(S, N, gl, Gc, eps2f);
 }
 
 struct EnsArgs {
@@ -289,7 +345,7 @@ struct EnsArgs {
 
 // A group of G lanes takes systems s in [lo, hi) from the counter and runs
 // `nsteps` reference ticks on each with its state in shared memory.
-template <int G, bool kExact, class S_t>
+template <int G, bool kExact, int kMaxTC, class S_t>
 __device__ void drain(S_t* S, const EnsArgs& a, int lo, int hi, int* ctr, int maxn) {
   const int gl = (threadIdx.x & 31) % G;
   const unsigned gm = group_mask<G>();
@@ -303,8 +359,8 @@ __device__ void drain(S_t* S, const EnsArgs& a, int lo, int hi, int* ctr, int ma
     const int sys = a.order[s];
     const int64_t b = a.off[sys];
     const int N = (int)(a.off[sys + 1] - b);
-    // odd N uses slot N as a pad: N < maxn, or N == maxn when even
-    if (N < 0 || N > maxn || ((N & 1) && N == maxn)) {
+    // slots up to N rounded up to 4 are used (maxn is a multiple of 4)
+    if (N < 0 || N > maxn) {
       if (gl == 0) atomicOr(a.status, kStatOverflow);
       continue;
     }
@@ -321,9 +377,10 @@ __device__ void drain(S_t* S, const EnsArgs& a, int lo, int hi, int* ctr, int ma
       S->m[i] = a.m[b + i];
       split_into(S, i);
     }
-    if ((N & 1) && gl == 0) set_pad(S, N);
+    // slots N .. N rounded up to 4 are massless pads (the quads of sources)
+    for (int i = N + gl; i < ((N + 3) & ~3); i += G) set_pad(S, i);
     __syncwarp(gm);
-    if (a.need_accel && N >= 2) group_forces<G, kExact>(S, N, gl, a.Gc, a.eps2);
+    if (a.need_accel && N >= 2) group_forces<G, kExact, kMaxTC>(S, N, gl, a.Gc, a.eps2);
     if (a.need_accel && N < 2)
       for (int i = gl; i < N; i += G) S->ax[i] = S->ay[i] = S->az[i] = 0.0;
     __syncwarp(gm);
@@ -340,7 +397,7 @@ __device__ void drain(S_t* S, const EnsArgs& a, int lo, int hi, int* ctr, int ma
         split_into(S, i);
       }
       __syncwarp(gm);
-      if (N >= 2) group_forces<G, kExact>(S, N, gl, a.Gc, a.eps2);
+      if (N >= 2) group_forces<G, kExact, kMaxTC>(S, N, gl, a.Gc, a.eps2);
       __syncwarp(gm);
       // velocity_verlet_velocity_system: v += (prev + a) dt/2
       for (int i = gl; i < N; i += G) {
@@ -379,13 +436,13 @@ ensemble_kernel(EnsArgs a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if constexpr (G != 0) {
     GroupSmem* S = reinterpret_cast<GroupSmem*>(smem_raw) + warp * (32 / G) + lane / G;
-    drain<G, kExact>(S, a, 0, a.nsys, a.queue, kMaxSys);
+    drain<G, kExact, (G == 32 ? 1 : 2)>(S, a, 0, a.nsys, a.queue, kMaxSys);
   } else {
     unsigned char* base = smem_raw + warp * sizeof(GroupSmem);
-    drain<32, kExact>(reinterpret_cast<GroupSmem*>(base), a, 0, a.n32, a.queue, kMaxSys);
-    drain<16, kExact>(reinterpret_cast<GroupSmemT<16>*>(base) + (lane >> 4), a, a.n32, a.n16,
+    drain<32, kExact, 1>(reinterpret_cast<GroupSmem*>(base), a, 0, a.n32, a.queue, kMaxSys);
+    drain<16, kExact, 1>(reinterpret_cast<GroupSmemT<16>*>(base) + (lane >> 4), a, a.n32, a.n16,
                       a.queue + 1, 16);
-    drain<8, kExact>(reinterpret_cast<GroupSmemT<8>*>(base) + (lane >> 3), a, a.n16, a.nsys,
+    drain<8, kExact, 1>(reinterpret_cast<GroupSmemT<8>*>(base) + (lane >> 3), a, a.n16, a.nsys,
                      a.queue + 2, 8);
   }
 }
