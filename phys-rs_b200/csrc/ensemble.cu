@@ -22,6 +22,9 @@ namespace {
 
 constexpr int kMaxSys = 64;        // bodies per system
 constexpr int kEnsCandidates = PHYS_ENS_CANDIDATES;
+// F32C: sources per partial sum before it is folded into the compensated
+// (hi, lo) accumulator (a system has at most 64)
+constexpr int kFold = 32;
 
 // Per-group state in shared memory for systems of at most MAXN bodies.
 template <int MAXN>
@@ -133,7 +136,7 @@ __device__ __forceinline__ TargetNeg target_neg(const S_t* S, int i) {
 // F32C accelerations of the group's own targets, TC targets per pass.  The
 // sources come four at a time (two packed f32x2 pairs: sources j, j+1 and
 // j+2, j+3); with one target per lane the two pairs go to separate partial
-// sums, so two dependency chains interleave.  Partial sums of 16 sources are
+// sums, so two dependency chains interleave.  Partial sums of kFold sources are
 // folded into a (hi, lo) accumulator by two-sum.
 template <int G, int TC, bool kSkip, class S_t>
 __device__ void group_forces_f32c(S_t* S, int N, int gl, double Gc, float eps2f) {
@@ -153,8 +156,8 @@ __device__ void group_forces_f32c(S_t* S, int N, int gl, double Gc, float eps2f)
 #pragma unroll
       for (int k = 0; k < kSets; ++k) px[k][t] = py[k][t] = pz[k][t] = make_float2(0.f, 0.f);
     }
-    for (int j0 = 0; j0 < n4; j0 += 16) {
-      const int j1 = min(n4, j0 + 16);
+    for (int j0 = 0; j0 < n4; j0 += kFold) {
+      const int j1 = min(n4, j0 + kFold);
       for (int j = j0; j < j1; j += 4) {
         const QuadSrc q = load_quad(S, j);
 #pragma unroll
@@ -230,7 +233,7 @@ __device__ void group_forces_f32c_split(S_t* S, int N, int gl, double Gc, float 
       pair_term<kSkip>(hi2(q.sx), hi2(q.sy), hi2(q.sz), hi2(q.sm), hi2(q.tx), hi2(q.ty),
                        hi2(q.tz), A.hx, A.hy, A.hz, A.lx, A.ly, A.lz, e2, j + 2 == ta,
                        j + 3 == ta, pax1, pay1, paz1);
-      if (++fa == 4) {
+      if (++fa == kFold / 4) {
         fold(pax0, hax, lax);
         fold(pay0, hay, lay);
         fold(paz0, haz, laz);
@@ -250,7 +253,7 @@ __device__ void group_forces_f32c_split(S_t* S, int N, int gl, double Gc, float 
       pair_term<kSkip>(hi2(q.sx), hi2(q.sy), hi2(q.sz), hi2(q.sm), hi2(q.tx), hi2(q.ty),
                        hi2(q.tz), B.hx, B.hy, B.hz, B.lx, B.ly, B.lz, e2, j + 2 == tbv,
                        j + 3 == tbv, pbx, pby, pbz);
-      if (++fb == 4) {
+      if (++fb == kFold / 4) {
         fold(pbx, hbx, lbx);
         fold(pby, hby, lby);
         fold(pbz, hbz, lbz);
