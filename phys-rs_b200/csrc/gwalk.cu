@@ -64,9 +64,6 @@
 #ifndef GWALK_SPLIT
 #define GWALK_SPLIT 1
 #endif
-#ifndef GWALK_EXACT_MIN
-#define GWALK_EXACT_MIN 0
-#endif
 #ifndef GWALK_FAR
 #define GWALK_FAR 0.0625
 #endif
@@ -107,9 +104,7 @@ constexpr int kGListOff = kGStack * 4;
 constexpr int kGRecOff = kGListOff + kGList * 32;
 constexpr int kGSmemWarp = kGRecOff + 5 * 32 * 4 + 32 * 32;
 constexpr int kGSmem = kGWarps * kGSmemWarp;
-// list kernel, per warp: stack | the group's bodies (f32 offsets)
-constexpr int kLSmemWarp = kGStack * 4 + kGroupMax * 16;
-constexpr int kLSmem = kLWarps * kLSmemWarp;
+constexpr int kLSmem = kLWarps * kGStack * 4;  // list kernel: stacks
 // evaluation kernel, per warp: near list (7 arrays) | far list (4 arrays) of
 // kEB entries, then two staging buffers of kEB source records
 #ifndef GEVAL_BATCH
@@ -189,9 +184,6 @@ __device__ __forceinline__ void two_sum2(float2 a, float2 b, float2& s, float2& 
 struct Box {
   float cx, cy, cz, bx, by, bz;  // centre and half extent, relative to X0
   float hx, lx, hy, ly, hz, lz;  // X0 as double-float
-  // the group's bodies as f32 offsets from X0 (npts of them; 0: box only)
-  const float4* pts = nullptr;
-  int npts = 0;
 };
 
 // Warp-collective: box of the targets ta, tb of every lane (idle lanes pass
@@ -264,29 +256,6 @@ __device__ __forceinline__ void classify(int nd, int base, int gend, int nnodes,
     const float dz = fmaxf(fabsf(rz - B.cz) - B.bz, 0.f);
     const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     acc = lo.w < theta2f * d2 * (1.0f - 1e-5f);
-  }
-  if (GWALK_EXACT_MIN && !acc && !overlap && B.npts > 1) {
-    // the box's nearest point may be far from every body: take the cell if
-    // the reference criterion holds at every body of the group (with the
-    // same margin toward opening), the conjunction of the per-body walks'
-    // decisions
-    const float rx = (h.x - B.hx) + (lo.x - B.lx);
-    const float ry = (h.y - B.hy) + (lo.y - B.ly);
-    const float rz = (h.z - B.hz) + (lo.z - B.lz);
-    const float t2 = theta2f * (1.0f - 1e-5f);
-    // every body lies within |b| of the box centre: no body is farther than
-    // |com - c| + |b| from the centre of mass, so below that bound the cell
-    // is opened without the loop
-    const float ux = rx - B.cx, uy = ry - B.cy, uz = rz - B.cz;
-    const float far = sqrtf(fmaf(ux, ux, fmaf(uy, uy, uz * uz))) +
-                      sqrtf(fmaf(B.bx, B.bx, fmaf(B.by, B.by, B.bz * B.bz)));
-    bool all = lo.w < t2 * far * far * (1.0f + 1e-5f);
-    for (int k = 0; k < B.npts && all; ++k) {
-      const float4 q = B.pts[k];
-      const float ex = rx - q.x, ey = ry - q.y, ez = rz - q.z;
-      all = lo.w < t2 * fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-    }
-    acc = all;
   }
   if (acc) {
     o.nent = 1;
@@ -936,8 +905,7 @@ glist_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __rest
   if (sort_failed(status)) return;  // records built on an unfinished sort
   extern __shared__ __align__(16) unsigned char gsm[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int* stk = reinterpret_cast<int*>(gsm + wid * kLSmemWarp);
-  float4* pts = reinterpret_cast<float4*>(gsm + wid * kLSmemWarp + kGStack * 4);
+  int* stk = reinterpret_cast<int*>(gsm) + wid * kGStack;
   const int64_t region0 = (blockIdx.x * (int64_t)kLWarps + wid) * pool_per_warp;
   uint32_t* region = pool + region0;
   const int cap = (int)min64(pool_per_warp, (int64_t)INT_MAX);
@@ -958,17 +926,7 @@ glist_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __rest
     const int ia = base + 2 * lane, ib = ia + 1;
     const double4 ta = ia < gend ? body64[ia] : X0;
     const double4 tb = ib < gend ? body64[ib] : X0;
-    Box B = group_box(X0, ta, tb);
-    if (GWALK_EXACT_MIN) {
-      if (ia < gend)
-        pts[ia - base] = make_float4((float)(ta.x - X0.x), (float)(ta.y - X0.y),
-                                     (float)(ta.z - X0.z), 0.f);
-      if (ib < gend)
-        pts[ib - base] = make_float4((float)(tb.x - X0.x), (float)(tb.y - X0.y),
-                                     (float)(tb.z - X0.z), 0.f);
-      B.pts = pts;
-      B.npts = gend - base;  // traverse's first __syncwarp publishes them
-    }
+    const Box B = group_box(X0, ta, tb);
     int used = 0;
     auto sink = [&](int etot, int eoff, const NodeOut& o) -> bool {
       if (roff + used + etot > cap) return false;  // region full: re-queue
