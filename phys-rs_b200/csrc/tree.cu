@@ -18,6 +18,7 @@
 //   otherwise              -> internal cells at depths L[p-1]+1 .. L[p],
 //                             leaf at max(L[p-1], L[p]) + 1
 // Pre-order = order of (start, depth), so node ids are a prefix sum.
+#include <climits>
 #include <vector>
 
 #include "bh.cuh"
@@ -358,6 +359,77 @@ emit_nodes_kernel(int64_t n, const uint64_t* __restrict__ hs, const uint64_t* __
       int meta = d;
       if (leaf) meta |= kMetaLeaf;
       if (leaf && guard) meta |= kMetaGuard;
+      link[f + k] = make_int4(next, (int)p, (int)end, meta);
+    }
+  }
+}
+
+#ifndef TREE_PRUNED_EMIT
+#define TREE_PRUNED_EMIT 1
+#endif
+// Bucket leaves of capacity C > 1, emitted directly: a cell survives iff its
+// parent holds more than C bodies (the root always).  For sorted position p,
+// e*(p) = the deepest depth at which the cell holding p has more than C
+// bodies: C + 1 consecutive keys containing p share e octants iff the
+// minimum of their C adjacent common prefixes is >= e, so
+//   e*(p) = max over q in [p - C, p] of min(L[q], ..., L[q + C - 1])
+// (-1 when fewer than C + 1 keys exist).  Position p owns the cells at depths
+// Lp+1 .. dl (dl its leaf's depth in the full tree); of those it keeps the
+// ones no deeper than e*(p) + 1, and the deepest one kept is a leaf.
+__global__ void __launch_bounds__(kBlock)
+prune_count_kernel(int64_t n, const int32_t* __restrict__ L, const TreeHeader* __restrict__ hdr,
+                   int C, int32_t* __restrict__ cnt, int32_t* __restrict__ emax) {
+  const int D = hdr->dstar;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p <= n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    if (p == n) {
+      cnt[n] = 0;
+      continue;
+    }
+    int best = -1;
+    const int64_t q0 = p - C > 0 ? p - C : 0;
+    for (int64_t q = q0; q <= p && q + C <= n - 1; ++q) {
+      int m = INT_MAX;
+      for (int i = 0; i < C; ++i) m = min(m, L[q + i]);
+      best = max(best, m);
+    }
+    emax[p] = best;
+    const int Lp = p > 0 ? L[p - 1] : -1;
+    const int Ln = L[p];  // -1 for the last position
+    int c = 0;
+    if (Lp < D) {
+      const int dl = Ln >= D ? D : max(Lp, Ln) + 1;
+      c = max(0, min(dl, best + 1) - Lp);
+    }
+    cnt[p] = c;
+  }
+}
+
+__global__ void __launch_bounds__(kBlock)
+emit_pruned_kernel(int64_t n, const uint64_t* __restrict__ hs, const uint64_t* __restrict__ ls,
+                   const int32_t* __restrict__ L, const int32_t* __restrict__ cnt,
+                   const int32_t* __restrict__ first, const TreeHeader* __restrict__ hdr,
+                   int4* __restrict__ link) {
+  const int D = hdr->dstar;
+  const int32_t total = first[n];
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int c = cnt[p];
+    if (c == 0) continue;
+    const int32_t f = first[p];
+    const int Lp = p > 0 ? L[p - 1] : -1;
+    const int Ln = L[p];
+    const bool guard = Ln >= D;
+    const int dl = guard ? D : max(Lp, Ln) + 1;
+    for (int k = 0; k < c; ++k) {
+      const int d = Lp + 1 + k;
+      const bool full_leaf = d == dl;
+      const bool leaf = k == c - 1;
+      const int64_t end = (full_leaf && !guard) ? p + 1 : cell_end(n, hs, ls, p, d);
+      const int32_t next = end < n ? first[end] : total;
+      int meta = d;
+      if (leaf) meta |= kMetaLeaf;
+      if (full_leaf && guard) meta |= kMetaGuard;
       link[f + k] = make_int4(next, (int)p, (int)end, meta);
     }
   }
@@ -829,6 +901,14 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
               c->m, lo_s, body64, body_hi, body_lo, body2, c->d_status);
   PHYS_CUDA(c, cudaEventRecord(c->ev[5], c->stream));
   PHYS_LAUNCH(c, lcp_count_kernel, grid_for(n + 1), kBlock, 0, n, hs, lo_s, c->d_hdr, L, cnt);
+  // bucket leaves: count only the cells that survive (no full tree)
+  const bool pruned = p->leaf_cap > 1 && TREE_PRUNED_EMIT;
+  int32_t* emax = nullptr;
+  if (pruned) {
+    PHYS_TRY(ws_alloc(c, WS_NEWID, n + 1, &emax));
+    PHYS_LAUNCH(c, prune_count_kernel, grid_for(n + 1), kBlock, 0, n, L, c->d_hdr, p->leaf_cap,
+                cnt, emax);
+  }
   PHYS_TRY(scan_exclusive_i32(c, cnt, first, n + 1));
   // node count, header and status word back to the host: a key sort that
   // gave up a bounded wait ends the evaluation here, before any kernel
@@ -855,11 +935,16 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
   int32_t* nchild = nullptr;
   PHYS_TRY(ws_alloc(c, WS_ARRIVE, 2 * (nfull + 1), &nchild));
   int32_t* arrive = nchild + (nfull + 1);
-  PHYS_LAUNCH(c, emit_nodes_kernel, grid_for(n), kBlock, 0, n, hs, lo_s, L, cnt, first, c->d_hdr,
-              link_full);
+  if (pruned) {
+    PHYS_LAUNCH(c, emit_pruned_kernel, grid_for(n), kBlock, 0, n, hs, lo_s, L, cnt, first,
+                c->d_hdr, link_full);
+  } else {
+    PHYS_LAUNCH(c, emit_nodes_kernel, grid_for(n), kBlock, 0, n, hs, lo_s, L, cnt, first,
+                c->d_hdr, link_full);
+  }
   int4* link = link_full;
   int64_t nnodes = nfull;
-  if (p->leaf_cap > 1) {
+  if (p->leaf_cap > 1 && !pruned) {
     PHYS_LAUNCH(c, children_kernel, grid_for(nfull), kBlock, 0, nfull, link_full, parent, nchild,
                 c->d_status);
     int32_t* keep = nullptr;
