@@ -139,7 +139,7 @@ enum WsSlot {
   WS_LCP, WS_NCOUNT, WS_NFIRST, WS_SCAN_TMP,
   WS_LINK, WS_NODE_PM, WS_NODE_HI, WS_NODE_LO, WS_PARENT, WS_ARRIVE, WS_NODE_S,
   WS_BODY_PM, WS_BODY_HI, WS_BODY_LO,
-  WS_KEEP, WS_NEWID, WS_LINK2,
+  WS_KEEP, WS_NEWID,
   WS_ENTRIES, WS_ENTRIES_ALT, WS_EOFF,
   WS_DIRECT_PART, WS_ADJ0, WS_ADJ1, WS_ADJ2, WS_ADJ3, WS_ADJ4,
   WS_ENS0, WS_ENS1, WS_ENS2, WS_ENS3, WS_ENS4, WS_ENS5, WS_ENS6, WS_ENS7,

@@ -98,6 +98,10 @@ constexpr int kGFlushPairs = GWALK_FLUSH_PAIRS;
 constexpr int kEvalUnroll = GEVAL_UNROLL;  // 4-entry chunks in flight per lane
 constexpr int kGListLimit = GWALK_LIST_LIMIT;  // first-pass budget (typical lists: 3-4k)
 constexpr int kGSplit = GWALK_SPLIT;            // bodies per re-queued subgroup
+// list codes a region must have free before a walk starts: the first-pass
+// budget plus one round's entries (32 cells, bucket leaves of at most
+// kMaxLeafCap bodies) and slack
+constexpr int kGRegionNeed = kGListLimit + 32 * kMaxLeafCap + 64;
 // fused kernel, per warp: stack | list | emission records (end, kind, a, olo,
 // ohi and the source double4 per lane)
 constexpr int kGListOff = kGStack * 4;
@@ -900,15 +904,17 @@ __global__ void __launch_bounds__(kLBlock, GLIST_MIN_BLOCKS)
 glist_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __restrict__ groups,
              const int32_t* __restrict__ ngroups_p, int32_t* __restrict__ ctr,
              const double4* __restrict__ body64, float theta2f, uint32_t* __restrict__ pool,
-             int64_t pool_per_warp, int4* __restrict__ items, int32_t* __restrict__ nitems,
-             int2* __restrict__ retry, int32_t* __restrict__ nretry, int32_t* status) {
+             int64_t pool_per_warp, int64_t nspill, int32_t* __restrict__ spill_ctr,
+             int4* __restrict__ items, int32_t* __restrict__ nitems, int2* __restrict__ retry,
+             int32_t* __restrict__ nretry, int32_t* status) {
   if (sort_failed(status)) return;  // records built on an unfinished sort
   extern __shared__ __align__(16) unsigned char gsm[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   int* stk = reinterpret_cast<int*>(gsm) + wid * kGStack;
-  const int64_t region0 = (blockIdx.x * (int64_t)kLWarps + wid) * pool_per_warp;
+  const int64_t warps = (int64_t)gridDim.x * kLWarps;
+  int64_t region0 = (blockIdx.x * (int64_t)kLWarps + wid) * pool_per_warp;
   uint32_t* region = pool + region0;
-  const int cap = (int)min64(pool_per_warp, (int64_t)INT_MAX);
+  int cap = (int)min64(pool_per_warp, (int64_t)INT_MAX);
   int64_t* offs = reinterpret_cast<int64_t*>(items + n);
   const int ngroups = min(*ngroups_p, n);
   int roff = 0;  // used part of the region
@@ -922,6 +928,20 @@ glist_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __rest
       break;
     }
     const int base = gr.x, gend = gr.y;
+    if (cap - roff < kGRegionNeed) {
+      // too little room left for a list of the largest length: continue in
+      // a fresh spill region, so that whether a group is re-queued depends
+      // on its list alone, not on which groups this warp took before
+      int sreg = 0;
+      if (lane == 0) sreg = atomicAdd(spill_ctr, 1);
+      sreg = __shfl_sync(kFull, sreg, 0);
+      if (sreg < nspill) {
+        region0 = warps * pool_per_warp + sreg * (int64_t)kGRegionNeed;
+        region = pool + region0;
+        cap = kGRegionNeed;
+        roff = 0;
+      }
+    }
     const double4 X0 = body64[base];
     const int ia = base + 2 * lane, ib = ia + 1;
     const double4 ta = ia < gend ? body64[ia] : X0;
@@ -929,7 +949,9 @@ glist_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __rest
     const Box B = group_box(X0, ta, tb);
     int used = 0;
     auto sink = [&](int etot, int eoff, const NodeOut& o) -> bool {
-      if (roff + used + etot > cap) return false;  // region full: re-queue
+      // full (spill regions exhausted, or a guard leaf of very many bodies):
+      // re-queue
+      if (roff + used + etot > cap) return false;
       uint32_t* dst = region + roff + used + eoff;
       if (o.kind == 1) {
         dst[0] = (uint32_t)o.a << 1;
@@ -1149,21 +1171,23 @@ int launch(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force, 
   const int grid_fused = (int)min64((int64_t)sms * occ_fused, ceil_div(n, (int64_t)kGWarps));
   // list pool: one region per list warp, each at least one full list
   const int64_t warps = (int64_t)grid_list * kLWarps;
-  const int64_t pool_per_warp = std::max((int64_t)kGListLimit + 64,
+  const int64_t pool_per_warp = std::max((int64_t)kGRegionNeed,
                                          ceil_div(n * (int64_t)GWALK_POOL_PER_BODY, warps));
+  const int64_t nspill = warps;  // spill regions of kGRegionNeed codes, one per warp
   uint32_t* pool = nullptr;
   int4* items = nullptr;  // n int4 items, then n int64 pool offsets
-  PHYS_TRY(ws_alloc(c, WS_GROUP_POOL, warps * pool_per_warp, &pool));
+  PHYS_TRY(ws_alloc(c, WS_GROUP_POOL, warps * pool_per_warp + nspill * kGRegionNeed, &pool));
   PHYS_TRY(ws_alloc(c, WS_GROUP_ITEMS, 2 * n, &items));
   // group_ctr: [0] list counter, [1] re-queued count, [2] items, [3]
-  // evaluation counter, [4] second-walk counter
+  // evaluation counter, [4] second-walk counter, [5] spill regions taken
   int32_t* ctr = t.group_ctr;
-  PHYS_CUDA(c, cudaMemsetAsync(ctr, 0, 5 * sizeof(int32_t), c->stream));
+  PHYS_CUDA(c, cudaMemsetAsync(ctr, 0, 6 * sizeof(int32_t), c->stream));
   const double eps2 = p->eps * p->eps;
   const float theta2f = (float)(p->theta * p->theta);
   int2* retry = const_cast<int2*>(t.groups) + n;
   PHYS_LAUNCH(c, glist_kernel, grid_list, kLBlock, kLSmem, (int)n, (int)t.nnodes, t.gnode,
-              t.groups, t.ngroups, ctr, t.body64, theta2f, pool, pool_per_warp, items, ctr + 2,
+              t.groups, t.ngroups, ctr, t.body64, theta2f, pool, pool_per_warp, nspill, ctr + 5,
+              items, ctr + 2,
               retry, ctr + 1, c->d_status);
   // The re-queued subgroups (a few hundred serial, latency-bound walks at
   // most) run on the side stream beside the list evaluation; it is launched

@@ -364,9 +364,6 @@ emit_nodes_kernel(int64_t n, const uint64_t* __restrict__ hs, const uint64_t* __
   }
 }
 
-#ifndef TREE_PRUNED_EMIT
-#define TREE_PRUNED_EMIT 1
-#endif
 // Bucket leaves of capacity C > 1, emitted directly: a cell survives iff its
 // parent holds more than C bodies (the root always).  For sorted position p,
 // e*(p) = the deepest depth at which the cell holding p has more than C
@@ -456,40 +453,6 @@ children_kernel(int64_t nnodes, const int4* __restrict__ link, int32_t* __restri
       if (ch < lk.x) atomicOr(status, kStatOverflow);
     }
     nchild[k] = cc;
-  }
-}
-
-// Bucket leaves: keep a node iff its parent holds more than `cap` bodies.
-__global__ void keep_kernel(int64_t nnodes, const int4* __restrict__ link,
-                            const int32_t* __restrict__ parent, int cap,
-                            int32_t* __restrict__ keep) {
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k <= nnodes;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    if (k == nnodes) {
-      keep[k] = 0;
-      continue;
-    }
-    if (k == 0) {
-      keep[0] = 1;
-      continue;
-    }
-    const int4 pl = link[parent[k]];
-    keep[k] = (pl.z - pl.y) > cap ? 1 : 0;
-  }
-}
-
-__global__ void compact_kernel(int64_t nnodes, const int4* __restrict__ link,
-                               const int32_t* __restrict__ keep, const int32_t* __restrict__ newid,
-                               int cap, int4* __restrict__ out) {
-  const int32_t total = newid[nnodes];
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnodes;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    if (!keep[k]) continue;
-    const int4 lk = link[k];
-    const int32_t nx = lk.x >= nnodes ? total : newid[lk.x];
-    int meta = lk.w;
-    if ((lk.z - lk.y) <= cap) meta |= kMetaLeaf;
-    out[newid[k]] = make_int4(nx, lk.y, lk.z, meta);
   }
 }
 
@@ -843,7 +806,7 @@ __global__ void group_kernel(int64_t nnodes, const uint32_t* __restrict__ bfs2pr
 }  // namespace
 
 // Builds the tree for the current positions.  One host synchronisation reads
-// the node count (two with bucket leaves).
+// the node count (and the status word).
 int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool need_group,
              bool full_com) {
   const int64_t n = c->n;
@@ -902,7 +865,7 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
   PHYS_CUDA(c, cudaEventRecord(c->ev[5], c->stream));
   PHYS_LAUNCH(c, lcp_count_kernel, grid_for(n + 1), kBlock, 0, n, hs, lo_s, c->d_hdr, L, cnt);
   // bucket leaves: count only the cells that survive (no full tree)
-  const bool pruned = p->leaf_cap > 1 && TREE_PRUNED_EMIT;
+  const bool pruned = p->leaf_cap > 1;
   int32_t* emax = nullptr;
   if (pruned) {
     PHYS_TRY(ws_alloc(c, WS_NEWID, n + 1, &emax));
@@ -923,44 +886,24 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
   PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
   if (hsm[2] & kStatTimeout)
     return fail(c, PHYS_ERR_TIMEOUT, "radix sort of the descent keys: a bounded wait timed out");
-  int64_t nfull = hsm[0];
+  const int64_t nnodes = hsm[0];
   const int dstar = hsm[1];
-  if (nfull < 1 || nfull > (int64_t)n * (kMaxLevels + 1))
+  if (nnodes < 1 || nnodes > (int64_t)n * (kMaxLevels + 1))
     return fail(c, PHYS_ERR_CUDA, "tree build produced %lld nodes for %lld bodies",
-                (long long)nfull, (long long)n);
-  int4* link_full = nullptr;
-  PHYS_TRY(ws_alloc(c, WS_LINK2, nfull, &link_full));
+                (long long)nnodes, (long long)n);
+  int4* link = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_LINK, nnodes, &link));
   int32_t* parent = nullptr;
-  PHYS_TRY(ws_alloc(c, WS_PARENT, nfull + 1, &parent));
+  PHYS_TRY(ws_alloc(c, WS_PARENT, nnodes + 1, &parent));
   int32_t* nchild = nullptr;
-  PHYS_TRY(ws_alloc(c, WS_ARRIVE, 2 * (nfull + 1), &nchild));
-  int32_t* arrive = nchild + (nfull + 1);
+  PHYS_TRY(ws_alloc(c, WS_ARRIVE, 2 * (nnodes + 1), &nchild));
+  int32_t* arrive = nchild + (nnodes + 1);
   if (pruned) {
     PHYS_LAUNCH(c, emit_pruned_kernel, grid_for(n), kBlock, 0, n, hs, lo_s, L, cnt, first,
-                c->d_hdr, link_full);
+                c->d_hdr, link);
   } else {
     PHYS_LAUNCH(c, emit_nodes_kernel, grid_for(n), kBlock, 0, n, hs, lo_s, L, cnt, first,
-                c->d_hdr, link_full);
-  }
-  int4* link = link_full;
-  int64_t nnodes = nfull;
-  if (p->leaf_cap > 1 && !pruned) {
-    PHYS_LAUNCH(c, children_kernel, grid_for(nfull), kBlock, 0, nfull, link_full, parent, nchild,
-                c->d_status);
-    int32_t* keep = nullptr;
-    PHYS_TRY(ws_alloc(c, WS_KEEP, nfull + 1, &keep));
-    int32_t* newid = nullptr;
-    PHYS_TRY(ws_alloc(c, WS_NEWID, nfull + 1, &newid));
-    PHYS_LAUNCH(c, keep_kernel, grid_for(nfull + 1), kBlock, 0, nfull, link_full, parent,
-                p->leaf_cap, keep);
-    PHYS_TRY(scan_exclusive_i32(c, keep, newid, nfull + 1));
-    PHYS_CUDA(c, cudaMemcpyAsync(hsm, newid + nfull, sizeof(int32_t), cudaMemcpyDeviceToHost,
-                                 c->stream));
-    PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
-    nnodes = hsm[0];
-    PHYS_TRY(ws_alloc(c, WS_LINK, nnodes, &link));
-    PHYS_LAUNCH(c, compact_kernel, grid_for(nfull), kBlock, 0, nfull, link_full, keep, newid,
-                p->leaf_cap, link);
+                c->d_hdr, link);
   }
   PHYS_LAUNCH(c, children_kernel, grid_for(nnodes), kBlock, 0, nnodes, link, parent, nchild,
               c->d_status);
