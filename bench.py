@@ -252,10 +252,10 @@ def workload_config(args, precision, leaf_cap, walk="body"):
 # DRAM bytes (read + write) of one launch of the dominant kernel for the
 # default workload (N = 2^20 Plummer, theta 0.5, leaf capacity 8, F32C), each
 # from one ncu capture of this binary at full size:
-#   group walk, geval_kernel<true>: dram__bytes_read.sum 467.5 MB +
-#     dram__bytes_write.sum 52.0 MB;
+#   group walk, geval_kernel<true>: dram__bytes_read.sum 472.2 MB +
+#     dram__bytes_write.sum 53.5 MB;
 #   per-body walk, walk2_kernel: 131.8 MB + 25.3 MB.
-WALK_TRAFFIC_BYTES = {"group": 525.17e6, "body": 157.05e6}
+WALK_TRAFFIC_BYTES = {"group": 525.69e6, "body": 157.05e6}
 
 
 def walk_traffic(args):
