@@ -168,3 +168,24 @@ def test_mirror_system_group_walk_theta_zero(ctx):
                                       group_walk=True)
     physgpu.brute_force_gravity_system(wd, cfg, precision=F64, ctx=ctx)
     assert rel_err(wb.force, wd.force).max() < 1e-12
+
+
+@pytest.mark.parametrize("leaf_cap", [8, 16])
+def test_lists_do_not_depend_on_scheduling(ctx, leaf_cap):
+    """At 300 001 bodies a list warp's pool region holds about one group's
+    list, so which groups a warp takes decides whether its region fills;
+    a warp then continues in a spill region instead of re-queueing, so every
+    run builds the same lists: identical forces and interaction counts from
+    run to run, and the same count for F32C and F64."""
+    pos, _, m = ics.plummer(300001, seed=3)
+    ctx.upload(pos, None, m)
+    counts = {}
+    for prec in (F64, F32C):
+        p = make_params(1.0, 0.01, 0.5, BARNES_HUT, prec, leaf_cap, GROUP_WALK)
+        a1 = ctx.gravity_accel(p)
+        n1 = ctx.timings()["interactions"]
+        a2 = ctx.gravity_accel(p)
+        n2 = ctx.timings()["interactions"]
+        assert np.array_equal(a1, a2) and n1 == n2
+        counts[prec] = n1
+    assert counts[F64] == counts[F32C]
