@@ -402,6 +402,10 @@ prune_count_kernel(int64_t n, const int32_t* __restrict__ L, const TreeHeader* _
   }
 }
 
+// One thread per kept cell (the cells of one position can be many, each
+// with a search for its end: a thread per position would leave the long
+// chains near the root to a few threads).  Cell k belongs to the last
+// position p with first[p] <= k.
 __global__ void __launch_bounds__(kBlock)
 emit_pruned_kernel(int64_t n, const uint64_t* __restrict__ hs, const uint64_t* __restrict__ ls,
                    const int32_t* __restrict__ L, const int32_t* __restrict__ cnt,
@@ -409,26 +413,32 @@ emit_pruned_kernel(int64_t n, const uint64_t* __restrict__ hs, const uint64_t* _
                    int4* __restrict__ link) {
   const int D = hdr->dstar;
   const int32_t total = first[n];
-  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
-       p += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo = 0, hi = n - 1;  // largest p with first[p] <= k (first[n] = total > k)
+    while (lo < hi) {
+      const int64_t mid = (lo + hi + 1) >> 1;
+      if (first[mid] <= k)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const int64_t p = lo;
     const int c = cnt[p];
-    if (c == 0) continue;
-    const int32_t f = first[p];
+    const int kk = (int)(k - first[p]);
     const int Lp = p > 0 ? L[p - 1] : -1;
     const int Ln = L[p];
     const bool guard = Ln >= D;
     const int dl = guard ? D : max(Lp, Ln) + 1;
-    for (int k = 0; k < c; ++k) {
-      const int d = Lp + 1 + k;
-      const bool full_leaf = d == dl;
-      const bool leaf = k == c - 1;
-      const int64_t end = (full_leaf && !guard) ? p + 1 : cell_end(n, hs, ls, p, d);
-      const int32_t next = end < n ? first[end] : total;
-      int meta = d;
-      if (leaf) meta |= kMetaLeaf;
-      if (full_leaf && guard) meta |= kMetaGuard;
-      link[f + k] = make_int4(next, (int)p, (int)end, meta);
-    }
+    const int d = Lp + 1 + kk;
+    const bool full_leaf = d == dl;
+    const bool leaf = kk == c - 1;
+    const int64_t end = (full_leaf && !guard) ? p + 1 : cell_end(n, hs, ls, p, d);
+    const int32_t next = end < n ? first[end] : total;
+    int meta = d;
+    if (leaf) meta |= kMetaLeaf;
+    if (full_leaf && guard) meta |= kMetaGuard;
+    link[k] = make_int4(next, (int)p, (int)end, meta);
   }
 }
 
@@ -899,7 +909,7 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
   PHYS_TRY(ws_alloc(c, WS_ARRIVE, 2 * (nnodes + 1), &nchild));
   int32_t* arrive = nchild + (nnodes + 1);
   if (pruned) {
-    PHYS_LAUNCH(c, emit_pruned_kernel, grid_for(n), kBlock, 0, n, hs, lo_s, L, cnt, first,
+    PHYS_LAUNCH(c, emit_pruned_kernel, grid_for(nnodes), kBlock, 0, n, hs, lo_s, L, cnt, first,
                 c->d_hdr, link);
   } else {
     PHYS_LAUNCH(c, emit_nodes_kernel, grid_for(n), kBlock, 0, n, hs, lo_s, L, cnt, first,
