@@ -45,10 +45,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="bh",
-                    choices=["bh", "galaxy", "ensemble", "direct", "adjoint"],
-                    help="bh: 2^20 Plummer Barnes-Hut (default); galaxy: 2^24 disk+halo BH; "
-                         "ensemble: 16384 small systems; direct: 1024-body direct sum; "
-                         "adjoint: 4096-body trajectory gradient")
+                    choices=["bh", "galaxy", "ensemble", "direct", "adjoint", "bh_shared"],
+                    help="bh: 2^20 Plummer Barnes-Hut (default; one replica per GPU); "
+                         "galaxy: 2^24 disk+halo BH; ensemble: 16384 small systems; "
+                         "direct: 1024-body direct sum; adjoint: 4096-body trajectory "
+                         "gradient; bh_shared: one 2^20 Plummer system split by targets "
+                         "over the GPUs (all-gather of accelerations per evaluation)")
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--leaf-cap", type=int, default=8)
     ap.add_argument("--walk", default="group", choices=["body", "group"],
@@ -65,6 +67,7 @@ def parse():
     a = ap.parse_args()
     defaults = {  # n, theta, eps, dt per workload shape
         "bh": (1 << 20, 0.5, 0.01, 1e-3), "galaxy": (1 << 24, 0.6, 0.02, 5e-4),
+        "bh_shared": (1 << 20, 0.5, 0.01, 1e-3),
         "ensemble": (16384, 0.5, 1e-3, 1e-4), "direct": (1024, 0.5, 0.01, 1e-3),
         "adjoint": (4096, 0.5, 0.01, 1e-3)}[a.workload]
     a.n = a.n if a.n is not None else defaults[0]
@@ -530,15 +533,16 @@ def _line(args, ws, metric, value, unit, ms, dtype, config, **kw):
 
 
 def run_other(args, ws, rank, local):
-    """Ensemble, direct-sum and adjoint workload shapes (one device per rank).
-    The ensemble's systems are split over the ranks (strong scaling); the
-    direct and adjoint shapes run one independent replica per rank."""
+    """Ensemble, direct-sum, adjoint and shared Barnes-Hut workload shapes
+    (one device per rank).  The ensemble's systems are split over the ranks
+    and the shared system's targets too (strong scaling); the direct and
+    adjoint shapes run one independent replica per rank."""
     import torch
 
     import physgpu
     import physgpu.dist as dist
     import physgpu.ics as ics
-    from physgpu import DIRECT, F32C, F64, F64_EXACT, make_params
+    from physgpu import BARNES_HUT, DIRECT, F32C, F64, F64_EXACT, GROUP_WALK, make_params
 
     torch.cuda.set_device(local)
     if ws > 1:
@@ -659,6 +663,55 @@ def run_other(args, ws, rank, local):
                       "bench_step": "upload + 100 Velocity-Verlet ticks on the device"},
                      variants_ms_per_step={k: v[0] / args.steps for k, v in out.items()},
                      cpu_baseline=cpu, clocks=clk)
+    elif args.workload == "bh_shared":
+        # one system for the whole job, split by targets: every rank holds
+        # and integrates all bodies, builds the same tree, evaluates the
+        # groups of its share of the key order, and one all-gather of the
+        # shares' accelerations (24 bytes per body) completes each evaluation
+        n = args.n
+        pos, vel, m = ics.plummer(n, seed=0)
+        p = make_params(1.0, args.eps, args.theta, BARNES_HUT, F32C, args.leaf_cap, GROUP_WALK)
+        flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        ctx.upload(pos, vel, m)
+        ex = dist.SharedEvaluation(ctx)
+        ex.evaluate(p)
+
+        def tick():
+            ctx.vv_position_step(args.dt)
+            ex.evaluate(p)
+            ctx.vv_velocity_step(args.dt)
+        for _ in range(args.warmup):
+            tick()
+        barrier()
+        l0 = ctx.timings()["launches"]
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        clocks.start()
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                flush_buf.fill_(i & 0xff)
+                evs[i][0].record(stream)
+                tick()
+                evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        launches = ctx.timings()["launches"] - l0
+        ms = [a.elapsed_time(b) for a, b in evs]
+        t = dist.max_over_ranks(sum(ms), device="cuda")
+        value = n * args.steps / (t * 1e-3)
+        x_final, _, _ = ctx.download()
+        line = _line(args, ws, METRIC, value, "particle-steps/s", t / args.steps, "f32c",
+                     dict(workload_config(args, precision="f32c", leaf_cap=args.leaf_cap,
+                                          walk="group"),
+                          workload="barnes_hut_plummer_n%d_shared" % n,
+                          ics="Plummer a=1, equal masses 1/N, seed=0 (one system on all ranks)",
+                          parallelism="one system, targets split over %d rank(s) by key "
+                                      "order; all-gather of the shares' accelerations" % ws,
+                          l2="flushed between timed steps (256 MiB write)"),
+                     scaling="strong", clocks=clk, gpu_launches=launches,
+                     exchange_bytes_per_evaluation=24 * physgpu.share_chunk(n, ws) * ws,
+                     checksum_final_x=float(np.abs(x_final).sum()),
+                     note="same trajectory as one GPU bit for bit (tests/test_share_gpu.py)")
     elif args.workload == "adjoint":
         n, nsteps = args.n, args.adj_steps
         pos, vel, m = ics.plummer(n, seed=rank)
@@ -744,7 +797,7 @@ def main():
     args = parse()
     ws, rank, local = dist_env()
     if args.impl == "reference":
-        if args.workload in ("bh", "galaxy"):
+        if args.workload in ("bh", "galaxy", "bh_shared"):
             return run_reference(args, ws, rank)
         return run_reference_other(args, ws, rank)
     if args.workload in ("bh", "galaxy"):

@@ -191,6 +191,36 @@ int phys_gravity_accel(phys_ctx* ctx, const phys_params* p, double* ax, double* 
 int phys_direct_accel_targets(phys_ctx* ctx, const phys_params* p, int64_t nt,
                               const int64_t* targets, double* ax, double* ay, double* az);
 
+/* ---- target shares: one system split over GPUs ------------------------- */
+/* No counterpart in the reference (it runs on one CPU).  Every GPU holds the
+ * whole state (same upload, same integration), and each evaluates a share
+ * of the targets of the phys_gravity_accel evaluation: share `rank` of
+ * `world` covers targets [rank*c, min(n, (rank+1)*c)), c =
+ * phys_share_chunk(n, world) (a multiple of 128), by body index for the
+ * direct sum and by sorted (key-order) position for Barnes-Hut, whose every
+ * GPU builds the same tree.  The values equal a one-GPU evaluation's bit for
+ * bit: a target's sum does not depend on the share that computes it.
+ *
+ * phys_share_chunk: targets per share (-1 for n < 0 or world < 1). */
+int64_t phys_share_chunk(int64_t n, int32_t world);
+/* Evaluates share `rank` of `world` (accelerations a = F/m, with the NFW
+ * halo when one is set) and packs them into share_out, a DEVICE buffer of
+ * 3*c doubles on this context's device: ax | ay | az of the share's targets
+ * in target order, zero-padded to c.  Synchronous at return.  The caller
+ * then all-gathers the world blocks (rank r's block at offset r*3*c, e.g.
+ * ncclAllGather over NVLink, 24 bytes per body) and completes the
+ * evaluation with phys_gravity_accel_unshare before any other evaluation on
+ * this context. */
+int phys_gravity_accel_share(phys_ctx* ctx, const phys_params* p, int32_t rank, int32_t world,
+                             double* share_out);
+/* Scatters the gathered blocks (DEVICE buffer, world*3*c doubles) into the
+ * context's acceleration arrays for all n bodies and caches them as the
+ * evaluation's result (as phys_gravity_accel does), so that
+ * phys_vv_position_step / phys_vv_velocity_step continue from it.
+ * PHYS_ERR_STATE without a preceding share evaluation; PHYS_ERR_NONFINITE
+ * if a gathered value is not finite. */
+int phys_gravity_accel_unshare(phys_ctx* ctx, int32_t world, const double* gathered);
+
 /* ---- NFW phantom halo (src/physics/nfw.rs) ------------------------------ */
 /* NfwHaloConfig (nfw.rs:24-47): rho(r) = rho_0 / ((r/Rs)(1 + r/Rs)^2),
  * centred at `center` (local coordinates). */

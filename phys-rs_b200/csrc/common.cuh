@@ -78,6 +78,19 @@ struct phys_ctx {
   bool last_eval_bh = false;   // the interaction count lives in d_counter
   bool last_eval_group = false;  // ev[10], ev[11] bracket the group walk's list evaluation
 
+  // ---- target shares (one system split over GPUs) ----
+  // While share_hi >= 0 an evaluation computes only the targets [share_lo,
+  // share_hi): body indices for the direct sum, sorted (key-order) positions
+  // for Barnes-Hut.  share_world > 0 after phys_gravity_accel_share until the
+  // matching phys_gravity_accel_unshare (any other evaluation or a new
+  // upload clears it); share_perm is the sorted-to-index map of that
+  // evaluation's tree (the last tree's while evaluating; then a copy in a
+  // workspace slot that only the share entry points use).
+  int64_t share_lo = 0, share_hi = -1;
+  int32_t share_world = 0;
+  const uint32_t* share_perm = nullptr;
+  phys_params share_params{};
+
   // ---- batched ensemble (independent small systems) ----
   int64_t ens_nsys = 0, ens_nbody = 0;
   bool ens_accel_valid = false;
@@ -140,12 +153,13 @@ enum WsSlot {
   WS_LINK, WS_NODE_PM, WS_NODE_HI, WS_NODE_LO, WS_PARENT, WS_ARRIVE, WS_NODE_S,
   WS_BODY_PM, WS_BODY_HI, WS_BODY_LO,
   WS_KEEP, WS_NEWID,
-  WS_ENTRIES, WS_ENTRIES_ALT, WS_EOFF,
+  WS_ENTRIES, WS_ENTRIES_ALT, WS_EOFF, WS_ENTRY_BODY,
   WS_DIRECT_PART, WS_ADJ0, WS_ADJ1, WS_ADJ2, WS_ADJ3, WS_ADJ4,
   WS_ENS0, WS_ENS1, WS_ENS2, WS_ENS3, WS_ENS4, WS_ENS5, WS_ENS6, WS_ENS7,
-  WS_GROUPS, WS_GROUP_OFF, WS_GROUP_CTR, WS_GROUP_POOL, WS_GROUP_ITEMS,
+  WS_GROUPS, WS_GROUP_OFF, WS_GROUP_CTR, WS_GROUP_POOL, WS_GROUP_ITEMS, WS_SHARE_PERM,
   WS_COUNT_
 };
+static_assert(WS_COUNT_ <= sizeof(phys_ctx::ws) / sizeof(DevBuf), "workspace slots");
 
 // ---- kernels' host launchers (per .cu file) ----
 // nfw.cu (px/py/pz: the positions the halo acts on)
@@ -179,6 +193,10 @@ int bh_export(phys_ctx* c, const phys_params* p, int64_t cap, int64_t* nnodes, i
 int radix_sort_u64(phys_ctx* c, uint64_t* keys, uint32_t* vals, uint64_t* keys_alt,
                    uint32_t* vals_alt, int64_t n, int begin_bit, int end_bit, bool* result_in_alt);
 int scan_exclusive_i32(phys_ctx* c, const int32_t* in, int32_t* out, int64_t n);
+// share.cu (targets of one share into a block of 3 * chunk; all blocks back)
+int share_pack(phys_ctx* c, int64_t lo, int64_t hi, int64_t chunk, const uint32_t* perm,
+               double* out);
+int share_unpack(phys_ctx* c, int64_t chunk, const uint32_t* perm, const double* gathered);
 // verlet.cu
 int verlet_drift(phys_ctx* c, double dt);
 int verlet_kick(phys_ctx* c, double dt);
@@ -283,5 +301,21 @@ __device__ __forceinline__ void split_df(double v, float& hi, float& lo) {
 
 __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 __host__ __device__ inline int64_t min64(int64_t a, int64_t b) { return a < b ? a : b; }
+
+// Targets [lo, hi) of the current evaluation of n bodies: all of them unless
+// a target share is set (phys_gravity_accel_share).
+inline void target_range(const phys_ctx* c, int64_t n, int64_t& lo, int64_t& hi) {
+  lo = 0;
+  hi = n;
+  if (c->share_hi >= 0) {
+    lo = min64(c->share_lo, n);
+    hi = min64(c->share_hi, n);
+  }
+}
+// Targets per share when n bodies are split into `world` shares: a multiple
+// of 128 (the direct sum's tile), so that every share starts on a tile.
+inline int64_t share_chunk(int64_t n, int64_t world) {
+  return world > 0 ? ceil_div(ceil_div(n, world), 128) * 128 : 0;
+}
 
 }  // namespace phys

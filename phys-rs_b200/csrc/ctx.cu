@@ -187,6 +187,7 @@ int eval_gravity(phys_ctx* c, const phys_params* p, bool want_force) {
 // halo set, a = (F_gravity + F_nfw) / m (src/main.rs:109-110, nfw.rs:103-139,
 // integrators.rs:110-118).
 int eval(phys_ctx* c, const phys_params* p, bool want_force) {
+  c->share_world = 0;  // a pending share is void once anything else is evaluated
   // sector mode: positions flattened for this pass (the Barnes-Hut system's
   // per-body origin for Barnes-Hut, gravity_tree.rs:280-291)
   if (c->sector_mode) PHYS_TRY(sector_flatten(c, p->method == PHYS_BARNES_HUT));
@@ -426,6 +427,7 @@ int phys_state_upload(phys_ctx* c, int64_t n, const double* x, const double* y, 
   if (n > 0 && (!x || !y || !z || !m)) return fail(c, PHYS_ERR_ARG, "positions and masses are required");
   PHYS_TRY(ensure_state(c, n));
   c->n = n;
+  c->share_world = 0;  // a pending share's tree order belongs to the old state
   c->sector_mode = false;
   c->accel_valid = false;
   if (n == 0) return PHYS_OK;
@@ -457,6 +459,7 @@ int phys_state_upload_sectors(phys_ctx* c, int64_t n, const int64_t* sx, const i
     return fail(c, PHYS_ERR_ARG, "sectors, local positions and masses are required");
   PHYS_TRY(ensure_state(c, n));
   c->n = n;
+  c->share_world = 0;  // a pending share's tree order belongs to the old state
   c->sector_mode = false;
   c->accel_valid = false;
   if (n == 0) return PHYS_OK;
@@ -498,6 +501,7 @@ int phys_state_upload_sector_state(phys_ctx* c, int64_t n, const int64_t* sx, co
   PHYS_TRY(ensure_state(c, n));
   PHYS_TRY(sector_state_alloc(c, n));
   c->n = n;
+  c->share_world = 0;  // a pending share's tree order belongs to the old state
   c->sector_mode = true;
   c->sector_size = sector_size;
   c->accel_valid = false;
@@ -728,6 +732,76 @@ int phys_gravity_accel(phys_ctx* c, const phys_params* p, double* ax, double* ay
   int st = finish_status(c);
   c->tm.total_ms = ev_ms(c->ev[0], c->ev[1]);
   return st;
+}
+
+int64_t phys_share_chunk(int64_t n, int32_t world) {
+  return (n < 0 || world < 1) ? -1 : share_chunk(n, world);
+}
+
+int phys_gravity_accel_share(phys_ctx* c, const phys_params* p, int32_t rank, int32_t world,
+                             double* share_out) {
+  PHYS_ENTER(c);
+  PHYS_TRY(check_params(c, p));
+  if (c->n == 0) return fail(c, PHYS_ERR_STATE, "no body state uploaded");
+  if (world < 1 || rank < 0 || rank >= world)
+    return fail(c, PHYS_ERR_ARG, "share %d of %d", (int)rank, (int)world);
+  if (!share_out) return fail(c, PHYS_ERR_ARG, "share_out is required");
+  const int64_t n = c->n, chunk = share_chunk(n, world);
+  const int64_t lo = min64(n, (int64_t)rank * chunk), hi = min64(n, lo + chunk);
+  PHYS_TRY(reset_status(c));
+  // the evaluation writes the share's targets (and the rest of their
+  // groups); zero first, so that no target outside holds a stale or
+  // non-finite value
+  double* o[3] = {c->ax, c->ay, c->az};
+  if (c->halo_on) o[0] = c->fx, o[1] = c->fy, o[2] = c->fz;
+  for (double* a : o) PHYS_CUDA(c, cudaMemsetAsync(a, 0, sizeof(double) * n, c->stream));
+  PHYS_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+  c->share_lo = lo;
+  c->share_hi = hi;
+  const int st_eval = eval(c, p, false);
+  c->share_lo = 0;
+  c->share_hi = -1;
+  PHYS_TRY(st_eval);
+  uint32_t* perm = nullptr;
+  if (p->method == PHYS_BARNES_HUT && n >= 2) {
+    // keep the tree's order for the scatter in a slot of its own
+    PHYS_TRY(ws_alloc(c, WS_SHARE_PERM, n, &perm));
+    PHYS_CUDA(c, cudaMemcpyAsync(perm, c->share_perm, sizeof(uint32_t) * n,
+                                 cudaMemcpyDeviceToDevice, c->stream));
+  }
+  PHYS_TRY(share_pack(c, lo, hi, chunk, perm, share_out));
+  PHYS_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+  c->accel_valid = false;  // the acceleration arrays hold this share only
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  int st = finish_status(c);
+  c->tm.total_ms = ev_ms(c->ev[0], c->ev[1]);
+  if (st == PHYS_OK) {
+    c->share_world = world;
+    c->share_perm = perm;
+    c->share_params = *p;
+  }
+  return st;
+}
+
+int phys_gravity_accel_unshare(phys_ctx* c, int32_t world, const double* gathered) {
+  PHYS_ENTER(c);
+  if (c->share_world == 0)
+    return fail(c, PHYS_ERR_STATE, "no share evaluation to complete on this context");
+  if (world != c->share_world)
+    return fail(c, PHYS_ERR_ARG, "world %d differs from the share evaluation's %d", (int)world,
+                (int)c->share_world);
+  if (!gathered) return fail(c, PHYS_ERR_ARG, "gathered is required");
+  PHYS_TRY(reset_status(c));
+  PHYS_TRY(share_unpack(c, share_chunk(c->n, world), c->share_perm, gathered));
+  c->share_world = 0;
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  int32_t st = 0;
+  PHYS_TRY(read_status(c, &st));
+  if (st & kStatNonfinite)
+    return fail(c, PHYS_ERR_NONFINITE, "non-finite value in the gathered accelerations");
+  c->accel_valid = true;
+  c->accel_params = c->share_params;
+  return PHYS_OK;
 }
 
 int phys_direct_accel_targets(phys_ctx* c, const phys_params* p, int64_t nt,

@@ -19,13 +19,14 @@ namespace {
 constexpr int kExactBlock = 64;
 
 __global__ void __launch_bounds__(kExactBlock)
-direct_exact_kernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
-                    const double* __restrict__ z, const double* __restrict__ m, double G,
-                    double eps2, int want_force, double* __restrict__ ox,
-                    double* __restrict__ oy, double* __restrict__ oz, int32_t* status) {
+direct_exact_kernel(int64_t n, int64_t t0, int64_t t1, const double* __restrict__ x,
+                    const double* __restrict__ y, const double* __restrict__ z,
+                    const double* __restrict__ m, double G, double eps2, int want_force,
+                    double* __restrict__ ox, double* __restrict__ oy, double* __restrict__ oz,
+                    int32_t* status) {
   __shared__ double4 tile[kExactBlock];
-  const int64_t i = blockIdx.x * (int64_t)kExactBlock + threadIdx.x;
-  const bool valid = i < n;
+  const int64_t i = t0 + blockIdx.x * (int64_t)kExactBlock + threadIdx.x;
+  const bool valid = i < t1;
   double xi = 0, yi = 0, zi = 0, mi = 0;
   if (valid) {
     xi = x[i];
@@ -99,15 +100,15 @@ __device__ __forceinline__ void f64_tile(const double4* __restrict__ t, int cnt,
 }
 
 __global__ void __launch_bounds__(kTile)
-direct_f64_kernel(int64_t n, int64_t slice_len, const double* __restrict__ x,
-                  const double* __restrict__ y, const double* __restrict__ z,
-                  const double* __restrict__ m, double G, double eps2, int want_force,
-                  double* __restrict__ ox, double* __restrict__ oy, double* __restrict__ oz,
-                  double* __restrict__ part, int32_t* status) {
+direct_f64_kernel(int64_t n, int64_t t0, int64_t t1, int64_t slice_len,
+                  const double* __restrict__ x, const double* __restrict__ y,
+                  const double* __restrict__ z, const double* __restrict__ m, double G,
+                  double eps2, int want_force, double* __restrict__ ox, double* __restrict__ oy,
+                  double* __restrict__ oz, double* __restrict__ part, int32_t* status) {
   __shared__ double4 tile[kTile];
-  const int64_t tbase = blockIdx.x * (int64_t)kTile;
+  const int64_t tbase = t0 + blockIdx.x * (int64_t)kTile;  // t0: a multiple of kTile
   const int64_t i = tbase + threadIdx.x;
-  const bool valid = i < n;
+  const bool valid = i < t1;
   const double xi = valid ? x[i] : 0.0, yi = valid ? y[i] : 0.0, zi = valid ? z[i] : 0.0;
   const int64_t lo = blockIdx.y * slice_len;
   const int64_t hi = min64(n, lo + slice_len);
@@ -192,15 +193,16 @@ __device__ __forceinline__ void f32_group(const float4* __restrict__ th,
 }
 
 __global__ void __launch_bounds__(kTile)
-direct_f32c_kernel(int64_t n, int64_t slice_len, const float4* __restrict__ bh,
-                   const float4* __restrict__ bl, const double* __restrict__ m, double G,
-                   float eps2, int want_force, double* __restrict__ ox, double* __restrict__ oy,
-                   double* __restrict__ oz, double* __restrict__ part, int32_t* status) {
+direct_f32c_kernel(int64_t n, int64_t t0, int64_t t1, int64_t slice_len,
+                   const float4* __restrict__ bh, const float4* __restrict__ bl,
+                   const double* __restrict__ m, double G, float eps2, int want_force,
+                   double* __restrict__ ox, double* __restrict__ oy, double* __restrict__ oz,
+                   double* __restrict__ part, int32_t* status) {
   __shared__ float4 th[kTile];
   __shared__ float4 tl[kTile];
-  const int64_t tbase = blockIdx.x * (int64_t)kTile;
+  const int64_t tbase = t0 + blockIdx.x * (int64_t)kTile;  // t0: a multiple of kTile
   const int64_t i = tbase + threadIdx.x;
-  const bool valid = i < n;
+  const bool valid = i < t1;
   float4 hi4 = valid ? bh[i] : make_float4(0, 0, 0, 0);
   float4 lo4 = valid ? bl[i] : make_float4(0, 0, 0, 0);
   const int64_t lo = blockIdx.y * slice_len;
@@ -253,12 +255,14 @@ direct_f32c_kernel(int64_t n, int64_t slice_len, const float4* __restrict__ bh,
   }
 }
 
-// Sum slice partials in slice order and apply G (and m_i for forces).
-__global__ void slice_reduce_kernel(int64_t n, int nslices, const double* __restrict__ part,
+// Sum slice partials in slice order and apply G (and m_i for forces), for
+// targets [t0, t1) of partials laid out with stride n per component.
+__global__ void slice_reduce_kernel(int64_t n, int64_t t0, int64_t t1, int nslices,
+                                    const double* __restrict__ part,
                                     const double* __restrict__ m, double G, int want_force,
                                     double* __restrict__ ox, double* __restrict__ oy,
                                     double* __restrict__ oz, int32_t* status) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+  for (int64_t i = t0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < t1;
        i += (int64_t)gridDim.x * blockDim.x) {
     double ax = 0.0, ay = 0.0, az = 0.0;
     for (int s = 0; s < nslices; ++s) {
@@ -361,9 +365,20 @@ int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, 
   const double eps2 = p->eps * p->eps;
   PHYS_CUDA(c, cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned long long), c->stream));
   PHYS_CUDA(c, cudaEventRecord(c->ev[6], c->stream));
+  // targets [t0, t1): all, or the share (t0 a multiple of kTile); the slices
+  // follow from n alone, so a target's sum does not depend on the share
+  int64_t t0 = 0, t1 = n;
+  target_range(c, n, t0, t1);
+  if (t0 % kTile) return fail(c, PHYS_ERR_ARG, "direct-sum share must start on a tile");
+  const int64_t nt = t1 - t0;
+  if (nt <= 0) {
+    PHYS_CUDA(c, cudaEventRecord(c->ev[7], c->stream));
+    c->tm.interactions = 0;
+    return PHYS_OK;
+  }
   if (p->precision == PHYS_F64_EXACT) {
-    PHYS_LAUNCH(c, direct_exact_kernel, (int)ceil_div(n, kExactBlock), kExactBlock, 0, n, c->x,
-                c->y, c->z, c->m, p->G, eps2, (int)want_force, ox, oy, oz, c->d_status);
+    PHYS_LAUNCH(c, direct_exact_kernel, (int)ceil_div(nt, kExactBlock), kExactBlock, 0, n, t0, t1,
+                c->x, c->y, c->z, c->m, p->G, eps2, (int)want_force, ox, oy, oz, c->d_status);
   } else {
     const int64_t slices = choose_slices(n);
     const int64_t slice_len = ceil_div(ceil_div(n, slices), kTile) * kTile;
@@ -374,10 +389,10 @@ int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, 
       part = (double*)ws_get(c, WS_DIRECT_PART, sizeof(double) * 3 * n * nsl, &st);
       if (st) return st;
     }
-    dim3 grid((unsigned)ceil_div(n, kTile), (unsigned)nsl);
+    dim3 grid((unsigned)ceil_div(nt, kTile), (unsigned)nsl);
     if (p->precision == PHYS_F64) {
-      PHYS_LAUNCH(c, direct_f64_kernel, grid, kTile, 0, n, slice_len, c->x, c->y, c->z, c->m, p->G,
-                  eps2, (int)want_force, ox, oy, oz, part, c->d_status);
+      PHYS_LAUNCH(c, direct_f64_kernel, grid, kTile, 0, n, t0, t1, slice_len, c->x, c->y, c->z,
+                  c->m, p->G, eps2, (int)want_force, ox, oy, oz, part, c->d_status);
     } else {
       float4* bh = (float4*)ws_get(c, WS_BODY_HI, sizeof(float4) * n, &st);
       if (st) return st;
@@ -386,17 +401,17 @@ int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, 
       int g = (int)min64(ceil_div(n, 256), 148 * 8);
       PHYS_LAUNCH(c, split_bodies_kernel, g, 256, 0, n, c->x, c->y, c->z, c->m, bh, bl,
                   c->d_status);
-      PHYS_LAUNCH(c, direct_f32c_kernel, grid, kTile, 0, n, slice_len, bh, bl, c->m, p->G,
-                  (float)eps2, (int)want_force, ox, oy, oz, part, c->d_status);
+      PHYS_LAUNCH(c, direct_f32c_kernel, grid, kTile, 0, n, t0, t1, slice_len, bh, bl, c->m,
+                  p->G, (float)eps2, (int)want_force, ox, oy, oz, part, c->d_status);
     }
     if (nsl > 1) {
-      int g = (int)min64(ceil_div(n, 256), 148 * 8);
-      PHYS_LAUNCH(c, slice_reduce_kernel, g, 256, 0, n, (int)nsl, part, c->m, p->G,
+      int g = (int)min64(ceil_div(nt, 256), 148 * 8);
+      PHYS_LAUNCH(c, slice_reduce_kernel, g, 256, 0, n, t0, t1, (int)nsl, part, c->m, p->G,
                   (int)want_force, ox, oy, oz, c->d_status);
     }
   }
   PHYS_CUDA(c, cudaEventRecord(c->ev[7], c->stream));
-  c->tm.interactions = (uint64_t)n * (uint64_t)(n - 1);
+  c->tm.interactions = (uint64_t)nt * (uint64_t)(n - 1);
   c->tm.bbox_ms = c->tm.keys_ms = c->tm.sort_ms = c->tm.tree_ms = 0.0;
   c->tm.nodes = 0;
   c->tm.max_depth = 0;
@@ -419,15 +434,15 @@ cudaError_t direct_accel_launch_scratch(cudaStream_t s, int64_t n, const double*
   dim3 grid((unsigned)ceil_div(n, kTile), (unsigned)nsl);
   const int g = (int)min64(ceil_div(n, 256), 148 * 8);
   if (precision == PHYS_F64) {
-    direct_f64_kernel<<<grid, kTile, 0, s>>>(n, slice_len, x, y, z, m, G, eps2, 0, ox, oy, oz,
-                                             part, status);
+    direct_f64_kernel<<<grid, kTile, 0, s>>>(n, 0, n, slice_len, x, y, z, m, G, eps2, 0, ox, oy,
+                                             oz, part, status);
   } else {
     split_bodies_kernel<<<g, 256, 0, s>>>(n, x, y, z, m, bh, bl, status);
-    direct_f32c_kernel<<<grid, kTile, 0, s>>>(n, slice_len, bh, bl, m, G, (float)eps2, 0, ox, oy,
-                                              oz, part, status);
+    direct_f32c_kernel<<<grid, kTile, 0, s>>>(n, 0, n, slice_len, bh, bl, m, G, (float)eps2, 0,
+                                              ox, oy, oz, part, status);
   }
   if (nsl > 1)
-    slice_reduce_kernel<<<g, 256, 0, s>>>(n, (int)nsl, part, m, G, 0, ox, oy, oz, status);
+    slice_reduce_kernel<<<g, 256, 0, s>>>(n, 0, n, (int)nsl, part, m, G, 0, ox, oy, oz, status);
   return cudaGetLastError();  // the launch error, if any (and clears it)
 }
 
@@ -452,8 +467,8 @@ int direct_targets(phys_ctx* c, const phys_params* p, int64_t nt, const int64_t*
               c->z, c->m, p->G, eps2, (int)exact, part, ox, oy, oz, c->d_status);
   if (!exact) {
     int g = (int)min64(ceil_div(nt, 256), 148 * 8);
-    PHYS_LAUNCH(c, slice_reduce_kernel, g, 256, 0, nt, (int)nsl, part, c->m, p->G, 0, ox, oy, oz,
-                c->d_status);
+    PHYS_LAUNCH(c, slice_reduce_kernel, g, 256, 0, nt, 0, nt, (int)nsl, part, c->m, p->G, 0, ox,
+                oy, oz, c->d_status);
   }
   return PHYS_OK;
 }

@@ -901,7 +901,8 @@ __device__ __forceinline__ bool requeue(int2 gr, int n, int2* retry, int32_t* nr
 // offsets.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kLBlock, GLIST_MIN_BLOCKS)
-glist_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __restrict__ groups,
+glist_kernel(int n, int q0, int q1, int nnodes, const GNode* __restrict__ gn,
+             const int2* __restrict__ groups,
              const int32_t* __restrict__ ngroups_p, int32_t* __restrict__ ctr,
              const double4* __restrict__ body64, float theta2f, uint32_t* __restrict__ pool,
              int64_t pool_per_warp, int64_t nspill, int32_t* __restrict__ spill_ctr,
@@ -928,6 +929,7 @@ glist_kernel(int n, int nnodes, const GNode* __restrict__ gn, const int2* __rest
       break;
     }
     const int base = gr.x, gend = gr.y;
+    if (gend <= q0 || base >= q1) continue;  // no target of the share [q0, q1)
     if (cap - roff < kGRegionNeed) {
       // too little room left for a list of the largest length: continue in
       // a fresh spill region, so that whether a group is re-queued depends
@@ -1185,7 +1187,13 @@ int launch(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force, 
   const double eps2 = p->eps * p->eps;
   const float theta2f = (float)(p->theta * p->theta);
   int2* retry = const_cast<int2*>(t.groups) + n;
-  PHYS_LAUNCH(c, glist_kernel, grid_list, kLBlock, kLSmem, (int)n, (int)t.nnodes, t.gnode,
+  // a share evaluates the groups that hold any of its targets (sorted
+  // positions [q0, q1)); their other bodies get the same values as on the
+  // rank that owns them
+  int64_t q0 = 0, q1 = n;
+  target_range(c, n, q0, q1);
+  PHYS_LAUNCH(c, glist_kernel, grid_list, kLBlock, kLSmem, (int)n, (int)q0, (int)q1,
+              (int)t.nnodes, t.gnode,
               t.groups, t.ngroups, ctr, t.body64, theta2f, pool, pool_per_warp, nspill, ctr + 5,
               items, ctr + 2,
               retry, ctr + 1, c->d_status);

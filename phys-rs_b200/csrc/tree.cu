@@ -559,22 +559,57 @@ expand_kernel(int64_t total, int64_t nnodes, const int32_t* __restrict__ eoff,
 }
 
 //
-// With skip_unused, a cell that no target can take as a monopole gets only
-// its mass (the same running sum) and a NaN centre of mass: a cell of side s
-// is taken only if s^2 < theta^2 |com - x|^2, and com and x both lie in the
-// root cube of half size H (com as a convex combination of bodies: every
-// mass positive, else nothing is skipped), so |com - x|^2 <= 12 H^2; when
-// s^2 >= theta^2 12 H^2 (with a 1e-6 margin for rounding) the walk opens the
-// cell whatever its centre of mass (a NaN distance opens it too).  This is
-// the root for theta <= 0.577 and every internal cell for theta = 0, and it
-// removes the longest chain of dependent divides (the root's, one per body).
+// With skip_unused, a cell that no target can take as a monopole is not
+// summed at all: a cell of side s is taken only if s^2 < theta^2 |com - x|^2,
+// and com and x both lie in the root cube of half size H (com as a convex
+// combination of bodies: every mass positive, else nothing is skipped), so
+// |com - x|^2 <= 12 H^2; when s^2 >= theta^2 12 H^2 (with a 1e-6 margin for
+// rounding) the walk opens the cell whatever its centre of mass (a NaN
+// distance opens it too).  Such a cell gets a NaN centre of mass and mass
+// +inf: nothing reads either, and a positive mass sets the same gate
+// (mass > 0) as the exact sum of positive masses.  This is the root for
+// theta <= 0.577 and every internal cell for theta = 0; it removes the
+// longest chains, the root's one step per body.
+__device__ __forceinline__ bool com_unused(bool can_skip, double bound, int4 lk,
+                                           const TreeHeader* __restrict__ hdr) {
+  return can_skip && !(lk.w & kMetaLeaf) && hdr->s2[lk.w & kMetaDepth] >= bound;
+}
+
+// Bodies of the (cell, body) pairs in pair order, so that each cell's
+// recurrence streams them from consecutive addresses (cells skipped by
+// com_unused are left out).
+__global__ void __launch_bounds__(kBlock)
+gather_entries_kernel(int64_t total, const uint64_t* __restrict__ entries,
+                      const double* __restrict__ x, const double* __restrict__ y,
+                      const double* __restrict__ z, const double* __restrict__ m,
+                      const int4* __restrict__ link, const TreeHeader* __restrict__ hdr,
+                      int skip_unused, double4* __restrict__ eb, const int32_t* status) {
+  if (sort_failed(status)) return;
+  const bool can_skip = skip_unused && hdr->min_mass > 0.0;
+  const double bound = hdr->theta2 * 12.0 * hdr->half * hdr->half * (1.0 + 1e-6);
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t v = entries[e];
+    if (com_unused(can_skip, bound, link[v >> 32], hdr)) continue;
+    const uint32_t b = (uint32_t)(v & 0xffffffffu);
+    eb[e] = make_double4(x[b], y[b], z[b], m[b]);
+  }
+}
+
+// Cells with at least kLongChain bodies run on a warp each
+// (com_recurrence_long_kernel), the rest on a thread each.
+constexpr int kLongChain = 2048;
+
+// One thread per cell runs the recurrence over the cell's gathered bodies;
+// the next batch's loads are issued before the current batch's chain of
+// dependent divides, so the chain (the critical path: a multiply, an add
+// and a divide per body) does not wait for memory.  Cells of kLongChain
+// bodies or more are appended to `longs` (count in longs[nnodes]) instead.
 __global__ void __launch_bounds__(kBlock)
 com_recurrence_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
-                      const uint64_t* __restrict__ entries, const double* __restrict__ x,
-                      const double* __restrict__ y, const double* __restrict__ z,
-                      const double* __restrict__ m, double4* __restrict__ mc,
+                      const double4* __restrict__ eb, double4* __restrict__ mc,
                       const int4* __restrict__ link, const TreeHeader* __restrict__ hdr,
-                      int skip_unused, const int32_t* status) {
+                      int skip_unused, int32_t* __restrict__ longs, const int32_t* status) {
   if (sort_failed(status)) return;
   // the bound holds when every centre of mass is a convex combination of
   // bodies (all masses positive)
@@ -583,41 +618,84 @@ com_recurrence_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnodes;
        k += (int64_t)gridDim.x * blockDim.x) {
     const int64_t e0 = eoff[k], e1 = eoff[k + 1];
-    double M = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
-    if (can_skip && !(link[k].w & kMetaLeaf) && hdr->s2[link[k].w & kMetaDepth] >= bound) {
-      for (int64_t e = e0; e < e1; ++e) M = xadd(M, m[(uint32_t)(entries[e] & 0xffffffffu)]);
-      mc[k] = make_double4(__longlong_as_double(0x7ff8000000000000ll),
-                           __longlong_as_double(0x7ff8000000000000ll),
-                           __longlong_as_double(0x7ff8000000000000ll), M);
+    if (com_unused(can_skip, bound, link[k], hdr)) {
+      const double nan = __longlong_as_double(0x7ff8000000000000ll);
+      mc[k] = make_double4(nan, nan, nan, __longlong_as_double(0x7ff0000000000000ll));
       continue;
     }
+    if (e1 - e0 >= kLongChain) {
+      longs[atomicAdd(&longs[nnodes], 1)] = (int32_t)k;
+      continue;
+    }
+    double M = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
     constexpr int kB = 8;
+    double4 cur[kB], nxt[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u)
+      cur[u] = e0 + u < e1 ? eb[e0 + u] : make_double4(0.0, 0.0, 0.0, 0.0);
     for (int64_t e = e0; e < e1; e += kB) {
-      double bx[kB], by[kB], bz[kB], bm[kB];
+#pragma unroll
+      for (int u = 0; u < kB; ++u)
+        nxt[u] = e + kB + u < e1 ? eb[e + kB + u] : make_double4(0.0, 0.0, 0.0, 0.0);
 #pragma unroll
       for (int u = 0; u < kB; ++u) {
         if (e + u < e1) {
-          const uint32_t b = (uint32_t)(entries[e + u] & 0xffffffffu);
-          bx[u] = x[b];
-          by[u] = y[b];
-          bz[u] = z[b];
-          bm[u] = m[b];
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < kB; ++u) {
-        if (e + u < e1) {
-          const double nt = xadd(M, bm[u]);
+          const double4 b = cur[u];
+          const double nt = xadd(M, b.w);
           if (nt > 0.0) {
-            cx = xdiv(xadd(xmul(cx, M), xmul(bx[u], bm[u])), nt);
-            cy = xdiv(xadd(xmul(cy, M), xmul(by[u], bm[u])), nt);
-            cz = xdiv(xadd(xmul(cz, M), xmul(bz[u], bm[u])), nt);
+            cx = xdiv(xadd(xmul(cx, M), xmul(b.x, b.w)), nt);
+            cy = xdiv(xadd(xmul(cy, M), xmul(b.y, b.w)), nt);
+            cz = xdiv(xadd(xmul(cz, M), xmul(b.z, b.w)), nt);
           }
           M = nt;
         }
       }
+#pragma unroll
+      for (int u = 0; u < kB; ++u) cur[u] = nxt[u];
     }
     mc[k] = make_double4(cx, cy, cz, M);
+  }
+}
+
+// The same recurrence for the cells listed by com_recurrence_kernel, a warp
+// per cell: the warp loads the next 32 bodies (one coalesced 1 KiB read)
+// while lanes 0, 1 and 2 run the x, y and z chains of the current 32 from
+// shared memory, each also running the mass sum (the same additions in the
+// same order, so the three agree).  Memory latency hides behind the chains.
+constexpr int kLongWarps = 4;
+__global__ void __launch_bounds__(32 * kLongWarps)
+com_recurrence_long_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
+                           const double4* __restrict__ eb, double4* __restrict__ mc,
+                           const int32_t* __restrict__ longs, const int32_t* status) {
+  if (sort_failed(status)) return;
+  __shared__ double4 buf[kLongWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nlong = min(longs[nnodes], (int32_t)nnodes);
+  for (int i = blockIdx.x * kLongWarps + w; i < nlong; i += gridDim.x * kLongWarps) {
+    const int k = longs[i];
+    const int64_t e0 = eoff[k], e1 = eoff[k + 1];
+    const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
+    double M = 0.0, cc = 0.0;  // lane j < 3: coordinate j
+    double4 v = e0 + lane < e1 ? eb[e0 + lane] : zero;
+    for (int64_t e = e0; e < e1; e += 32) {
+      buf[w][lane] = v;
+      __syncwarp();
+      v = e + 32 + lane < e1 ? eb[e + 32 + lane] : zero;
+      const int cnt = (int)min((int64_t)32, e1 - e);
+      if (lane < 3) {
+        const double* q = reinterpret_cast<const double*>(&buf[w][0]);
+#pragma unroll 8
+        for (int u = 0; u < cnt; ++u) {
+          const double p = q[4 * u + lane], mm = q[4 * u + 3];
+          const double nt = xadd(M, mm);
+          if (nt > 0.0) cc = xdiv(xadd(xmul(cc, M), xmul(p, mm)), nt);
+          M = nt;
+        }
+      }
+      __syncwarp();
+    }
+    const double cy = __shfl_sync(0xffffffffu, cc, 1), cz = __shfl_sync(0xffffffffu, cc, 2);
+    if (lane == 0) mc[k] = make_double4(cc, cy, cz, M);
   }
 }
 
@@ -756,7 +834,10 @@ static_assert(kGroupBuild >= 1 && kGroupBuild <= kGroupMax, "group size");
 
 // Target groups of the group walk: every cell with more than kGroupBuild
 // bodies splits its children into runs of consecutive children with at most
-// kGroupBuild bodies between them (a child with more starts its own groups);
+// kGroupBuild bodies between them, each run inside one half of the cell
+// along z (octants 0-3 or 4-7: a run across the middle, e.g. octants 3 and
+// 4, would join diagonal neighbours into a box as large as the cell); a
+// child with more starts its own groups;
 // a leaf with more (guard depth) is cut into chunks; a root with at most
 // kGroupBuild bodies is one group.  The groups partition the bodies into
 // key-contiguous ranges that each lie inside one cell.  Cells are taken in
@@ -768,6 +849,8 @@ static_assert(kGroupBuild >= 1 && kGroupBuild <= kGroupMax, "group size");
 template <bool kEmit>
 __global__ void group_kernel(int64_t nnodes, const uint32_t* __restrict__ bfs2pre,
                              const int4* __restrict__ link, const int32_t* __restrict__ nchild,
+                             const uint64_t* __restrict__ hs, const uint64_t* __restrict__ klo,
+                             const uint32_t* __restrict__ perm,
                              int32_t* __restrict__ cnt, const int32_t* __restrict__ off,
                              int2* __restrict__ out, int64_t cap, const int32_t* status) {
   if (sort_failed(status)) return;
@@ -790,20 +873,25 @@ __global__ void group_kernel(int64_t nnodes, const uint32_t* __restrict__ bfs2pr
     } else if (lk.w & kMetaLeaf) {
       for (int b = lk.y; b < lk.z; b += kGroupBuild) put(b, min(b + kGroupBuild, lk.z));
     } else {
-      int c = (int)k + 1, rb = -1, re = -1;
+      int c = (int)k + 1, rb = -1, re = -1, ob = 0;
       const int nc = nchild[k];
+      const int d = lk.w & kMetaDepth;
       for (int i = 0; i < nc && c < nnodes; ++i) {
         const int4 lc = link[c];
         const int cc = lc.z - lc.y;
+        // the child's octant: digit d of its first body's descent key
+        const int oc = d < 21 ? (int)((hs[lc.y] >> (60 - 3 * d)) & 7)
+                              : (int)((klo[perm[lc.y]] >> (54 - 3 * (d - 21))) & 7);
         if (cc > kGroupBuild) {
           if (rb >= 0) put(rb, re);
           rb = -1;
-        } else if (rb >= 0 && re - rb + cc <= kGroupBuild) {
+        } else if (rb >= 0 && (ob >> 2) == (oc >> 2) && re - rb + cc <= kGroupBuild) {
           re = lc.z;
         } else {
           if (rb >= 0) put(rb, re);
           rb = lc.y;
           re = lc.z;
+          ob = oc;
         }
         c = lc.x;
       }
@@ -946,8 +1034,18 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
     uint64_t* e1_alt = alt1 ? ent : ent_alt;
     PHYS_TRY(radix_sort_u64(c, e1, nullptr, e1_alt, nullptr, total, 32, 32 + bits_n, &alt2));
     uint64_t* es = alt2 ? e1_alt : e1;
-    PHYS_LAUNCH(c, com_recurrence_kernel, grid_for(nnodes, 128, 1 << 30), 128, 0, nnodes, eoff, es,
-                c->x, c->y, c->z, c->m, mc, link, c->d_hdr, full_com ? 0 : 1, c->d_status);
+    double4* eb = nullptr;
+    PHYS_TRY(ws_alloc(c, WS_ENTRY_BODY, total, &eb));
+    PHYS_LAUNCH(c, gather_entries_kernel, grid_for(total), kBlock, 0, total, es, c->x, c->y,
+                c->z, c->m, link, c->d_hdr, full_com ? 0 : 1, eb, c->d_status);
+    // the node counts are consumed by the scan: their array takes the list
+    // of long cells, its count in the last slot
+    int32_t* longs = ncnt;
+    PHYS_CUDA(c, cudaMemsetAsync(longs + nnodes, 0, sizeof(int32_t), c->stream));
+    PHYS_LAUNCH(c, com_recurrence_kernel, grid_for(nnodes, 128, 1 << 30), 128, 0, nnodes, eoff, eb,
+                mc, link, c->d_hdr, full_com ? 0 : 1, longs, c->d_status);
+    PHYS_LAUNCH(c, com_recurrence_long_kernel, 148 * 4, 32 * kLongWarps, 0, nnodes, eoff, eb, mc,
+                longs, c->d_status);
   } else {
     PHYS_CUDA(c, cudaMemsetAsync(arrive, 0, sizeof(int32_t) * (nnodes + 1), c->stream));
     PHYS_LAUNCH(c, com_upward_kernel, grid_for(nnodes), kBlock, 0, nnodes, link, parent, nchild,
@@ -997,10 +1095,10 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
     PHYS_TRY(ws_alloc(c, WS_GROUPS, 2 * n, &groups));  // groups, then re-queued subgroups
     PHYS_TRY(ws_alloc(c, WS_GROUP_CTR, 8, &gctr));
     PHYS_LAUNCH(c, group_kernel<false>, grid_for(nnodes + 1), kBlock, 0, nnodes, bfs2pre, link,
-                nchild, gcnt, goff, groups, n, c->d_status);
+                nchild, hs, klo, perm, gcnt, goff, groups, n, c->d_status);
     PHYS_TRY(scan_exclusive_i32(c, gcnt, goff, nnodes + 1));
     PHYS_LAUNCH(c, group_kernel<true>, grid_for(nnodes + 1), kBlock, 0, nnodes, bfs2pre, link,
-                nchild, gcnt, goff, groups, n, c->d_status);
+                nchild, hs, klo, perm, gcnt, goff, groups, n, c->d_status);
     t->groups = groups;
     t->ngroups = goff + nnodes;
     t->group_ctr = gctr;
@@ -1034,6 +1132,7 @@ int bh_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, doub
   // the exact form's forces need no centre of mass of cells no target can
   // take as a monopole
   PHYS_TRY(bh_build(c, p, p->precision == PHYS_F32C && !group, &t, group, false));
+  c->share_perm = t.perm;  // sorted position -> body, for a target share
   return bh_walk(c, p, t, want_force, ox, oy, oz);
 }
 

@@ -47,7 +47,7 @@ __device__ __forceinline__ void warp_count(unsigned ninter, unsigned long long* 
 
 template <bool kF32>
 __global__ void __launch_bounds__(kWalkBlock)
-walk_kernel(int n, int nnodes, const Rec32* __restrict__ w32, const Rec64* __restrict__ w64,
+walk_kernel(int q0, int n, int nnodes, const Rec32* __restrict__ w32, const Rec64* __restrict__ w64,
             const double4* __restrict__ body64, const float4* __restrict__ body_hi,
             const float4* __restrict__ body_lo, const uint32_t* __restrict__ perm,
             const TreeHeader* __restrict__ hdr, double G, double eps2, int want_force,
@@ -61,7 +61,7 @@ walk_kernel(int n, int nnodes, const Rec32* __restrict__ w32, const Rec64* __res
   }
   const double theta2 = hdr->theta2;
   const float eps2f = (float)eps2;
-  const int p = blockIdx.x * kWalkBlock + threadIdx.x;
+  const int p = q0 + blockIdx.x * kWalkBlock + threadIdx.x;  // targets [q0, n)
   const bool valid = p < n;
 
   double tx = 0, ty = 0, tz = 0;
@@ -252,12 +252,12 @@ __device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); 
 __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
 
 __global__ void __launch_bounds__(kWalk2Block)
-walk2_kernel(int n, int nnodes, const Rec32x2* __restrict__ w, const Body32x2* __restrict__ body2,
+walk2_kernel(int q0, int n, int nnodes, const Rec32x2* __restrict__ w, const Body32x2* __restrict__ body2,
              const double4* __restrict__ body64, const uint32_t* __restrict__ perm, double G,
              double eps2, int want_force, double* __restrict__ ox, double* __restrict__ oy,
              double* __restrict__ oz, unsigned long long* counter, int32_t* status) {
   const int lane = threadIdx.x & 31;
-  const int base = (blockIdx.x * (kWalk2Block / 32) + (threadIdx.x >> 5)) * 64;
+  const int base = q0 + (blockIdx.x * (kWalk2Block / 32) + (threadIdx.x >> 5)) * 64;
   const int pa = base + 2 * lane, pb = pa + 1;
   const bool va = pa < n, vb = pb < n;
   float2 nhx, nhy, nhz, nlx, nly, nlz;  // negated target coordinates (a, b)
@@ -375,7 +375,7 @@ walk2_kernel(int n, int nnodes, const Rec32x2* __restrict__ w, const Body32x2* _
 // F64_EXACT walk (leaf capacity 1).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kWalkBlock)
-walk_exact_kernel(int64_t n, int64_t nnodes, const int4* __restrict__ link,
+walk_exact_kernel(int64_t q0, int64_t n, int64_t nnodes, const int4* __restrict__ link,
                   const double4* __restrict__ rec64, const double4* __restrict__ body64,
                   const uint32_t* __restrict__ perm, const TreeHeader* __restrict__ hdr, double G,
                   double eps2, int want_force, double* __restrict__ ox, double* __restrict__ oy,
@@ -384,7 +384,7 @@ walk_exact_kernel(int64_t n, int64_t nnodes, const int4* __restrict__ link,
   for (int d = threadIdx.x; d < kMaxLevels; d += blockDim.x) s2d[d] = hdr->s2[d];
   __syncthreads();
   const double theta2 = hdr->theta2;
-  const int64_t p = blockIdx.x * (int64_t)kWalkBlock + threadIdx.x;
+  const int64_t p = q0 + blockIdx.x * (int64_t)kWalkBlock + threadIdx.x;  // targets [q0, n)
   const bool valid = p < n;
   double tx = 0, ty = 0, tz = 0, mi = 0;
   if (valid) {
@@ -477,25 +477,29 @@ int bh_walk(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force,
             double* oy, double* oz) {
   const int64_t n = t.n;
   const double eps2 = p->eps * p->eps;
-  const int grid = (int)ceil_div(n, kWalkBlock);
+  // targets: sorted positions [q0, q1), all or the share
+  int64_t q0 = 0, q1 = n;
+  target_range(c, n, q0, q1);
+  const int64_t nt = q1 > q0 ? q1 - q0 : 0;
+  const int grid = (int)ceil_div(nt > 0 ? nt : 1, kWalkBlock);
   PHYS_CUDA(c, cudaMemsetAsync(c->d_counter, 0, 2 * sizeof(unsigned long long), c->stream));
   PHYS_CUDA(c, cudaEventRecord(c->ev[6], c->stream));
   if (p->flags & PHYS_FLAG_GROUP_WALK) {
     PHYS_TRY(bh_group_walk(c, p, t, want_force, ox, oy, oz));
   } else if (p->precision == PHYS_F64_EXACT) {
-    PHYS_LAUNCH(c, walk_exact_kernel, grid, kWalkBlock, 0, n, t.nnodes, t.link, t.rec64, t.body64,
+    PHYS_LAUNCH(c, walk_exact_kernel, grid, kWalkBlock, 0, q0, q1, t.nnodes, t.link, t.rec64, t.body64,
                 t.perm, t.hdr, p->G, eps2, (int)want_force, ox, oy, oz, c->d_counter, c->d_status);
   } else if (p->precision == PHYS_F64) {
-    PHYS_LAUNCH(c, walk_kernel<false>, grid, kWalkBlock, 0, (int)n, (int)t.nnodes, t.w32, t.w64,
+    PHYS_LAUNCH(c, walk_kernel<false>, grid, kWalkBlock, 0, (int)q0, (int)q1, (int)t.nnodes, t.w32, t.w64,
                 t.body64, t.body_hi, t.body_lo, t.perm, t.hdr, p->G, eps2, (int)want_force, ox, oy,
                 oz, c->d_counter, c->d_status);
   } else if (WALK_PAIRED && t.w32x2) {
-    const int grid2 = (int)ceil_div(n, 64 * (kWalk2Block / 32));
-    PHYS_LAUNCH(c, walk2_kernel, grid2, kWalk2Block, 0, (int)n, (int)t.nnodes, t.w32x2, t.body2,
+    const int grid2 = (int)ceil_div(nt > 0 ? nt : 1, 64 * (kWalk2Block / 32));
+    PHYS_LAUNCH(c, walk2_kernel, grid2, kWalk2Block, 0, (int)q0, (int)q1, (int)t.nnodes, t.w32x2, t.body2,
                 t.body64, t.perm, p->G, eps2, (int)want_force, ox, oy, oz, c->d_counter,
                 c->d_status);
   } else {
-    PHYS_LAUNCH(c, walk_kernel<true>, grid, kWalkBlock, 0, (int)n, (int)t.nnodes, t.w32, t.w64,
+    PHYS_LAUNCH(c, walk_kernel<true>, grid, kWalkBlock, 0, (int)q0, (int)q1, (int)t.nnodes, t.w32, t.w64,
                 t.body64, t.body_hi, t.body_lo, t.perm, t.hdr, p->G, eps2, (int)want_force, ox, oy,
                 oz, c->d_counter, c->d_status);
   }

@@ -54,7 +54,8 @@ EXPORTED = [
     "phys_direct_accel_noalloc", "phys_adjoint_direct", "phys_trajectory_loss",
     "phys_nfw_density", "phys_nfw_enclosed_mass", "phys_nfw_circular_velocity",
     "phys_nfw_forces", "phys_set_nfw_halo", "phys_state_upload_sector_state",
-    "phys_state_download_sector_state", "phys_debug_set_wait_limit",
+    "phys_state_download_sector_state", "phys_debug_set_wait_limit", "phys_share_chunk",
+    "phys_gravity_accel_share", "phys_gravity_accel_unshare",
 ]
 
 
@@ -152,6 +153,9 @@ def load_library(path=None):
         "phys_state_download_sector_state": ([_VP, _I64, _I64, _I64, _D, _D, _D],
                                              ctypes.c_int),
         "phys_debug_set_wait_limit": ([_VP, i64], ctypes.c_int),
+        "phys_share_chunk": ([i64, i32], i64),
+        "phys_gravity_accel_share": ([_VP, P, i32, i32, _VP], ctypes.c_int),
+        "phys_gravity_accel_unshare": ([_VP, i32, _VP], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -176,6 +180,12 @@ def make_params(G, eps, theta=0.5, method=DIRECT, precision=F64_EXACT, leaf_cap=
                   int(flags))
 
 
+def share_chunk(n, world):
+    """Targets per share when n bodies are split into `world` shares
+    (phys_share_chunk): a multiple of 128."""
+    return int(load_library().phys_share_chunk(int(n), int(world)))
+
+
 class Context:
     """One device context: a CUDA stream plus device-resident body state."""
 
@@ -188,6 +198,7 @@ class Context:
                 device, self.lib.phys_status_string(st).decode()))
         self.h = h
         self.n = 0
+        self.device = int(device)
 
     def close(self):
         if getattr(self, "h", None):
@@ -336,6 +347,22 @@ class Context:
         self._check(self.lib.phys_gravity_accel(self.h, ctypes.byref(params),
                                                 *[_p(a) for a in A]), "phys_gravity_accel")
         return np.stack(A, axis=1) if download else None
+
+    # ---- target shares (one system over several GPUs) ----
+    def gravity_accel_share(self, params, rank, world, out_ptr):
+        """Evaluates share `rank` of `world` of the targets and packs its
+        accelerations into the device buffer at address out_ptr (3 *
+        share_chunk(n, world) float64 on this context's device)."""
+        self._check(self.lib.phys_gravity_accel_share(self.h, ctypes.byref(params), int(rank),
+                                                      int(world), _VP(int(out_ptr))),
+                    "phys_gravity_accel_share")
+
+    def gravity_accel_unshare(self, world, gathered_ptr):
+        """Scatters all shares' blocks (device buffer at gathered_ptr, world *
+        3 * share_chunk(n, world) float64) into the acceleration arrays."""
+        self._check(self.lib.phys_gravity_accel_unshare(self.h, int(world),
+                                                        _VP(int(gathered_ptr))),
+                    "phys_gravity_accel_unshare")
 
     def direct_accel_targets(self, params, targets):
         """f64 direct-sum accelerations for the given targets (all sources)."""

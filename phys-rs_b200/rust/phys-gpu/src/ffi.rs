@@ -129,6 +129,13 @@ extern "C" {
                                      targets: *const i64, ax: *mut f64, ay: *mut f64,
                                      az: *mut f64) -> c_int;
 
+    // ---- target shares: one system split over GPUs (device buffers) ----
+    pub fn phys_share_chunk(n: i64, world: i32) -> i64;
+    pub fn phys_gravity_accel_share(ctx: *mut phys_ctx, p: *const phys_params, rank: i32,
+                                    world: i32, share_out: *mut f64) -> c_int;
+    pub fn phys_gravity_accel_unshare(ctx: *mut phys_ctx, world: i32,
+                                      gathered: *const f64) -> c_int;
+
     // ---- NFW phantom halo ----
     pub fn phys_nfw_density(r: f64, rho_0: f64, rs: f64) -> f64;
     pub fn phys_nfw_enclosed_mass(r: f64, rho_0: f64, rs: f64) -> f64;

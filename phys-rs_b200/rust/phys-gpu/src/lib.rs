@@ -323,6 +323,29 @@ impl PhysGpu {
         Ok(a)
     }
 
+    /// Share `rank` of `world` of the acceleration evaluation
+    /// (phys_gravity_accel_share) for one system held whole by every GPU,
+    /// packed into `share_out`; the caller all-gathers the shares (NCCL)
+    /// and completes the evaluation with `accel_unshare`.
+    ///
+    /// # Safety
+    /// `share_out` must point to 3 * share_chunk(n, world) f64 of device
+    /// memory on this context's GPU.
+    pub unsafe fn accel_share(&mut self, p: &ffi::phys_params, rank: i32, world: i32,
+                              share_out: *mut f64) -> Result<()> {
+        self.check(ffi::phys_gravity_accel_share(self.raw(), p, rank, world, share_out))
+    }
+
+    /// Scatters the gathered shares into the acceleration state
+    /// (phys_gravity_accel_unshare).
+    ///
+    /// # Safety
+    /// `gathered` must point to world * 3 * share_chunk(n, world) f64 of
+    /// device memory on this context's GPU.
+    pub unsafe fn accel_unshare(&mut self, world: i32, gathered: *const f64) -> Result<()> {
+        self.check(ffi::phys_gravity_accel_unshare(self.raw(), world, gathered))
+    }
+
     /// nsteps Velocity-Verlet ticks on the device-resident state.
     pub fn verlet_steps(&mut self, p: &ffi::phys_params, dt: f64, nsteps: i64) -> Result<()> {
         self.check(unsafe { ffi::phys_verlet_steps(self.raw(), p, dt, nsteps) })
@@ -431,6 +454,13 @@ fn arg_error(msg: &str) -> PhysError {
 }
 
 /// The library's name for a status code.
+/// Targets per share when `n` bodies are split over `world` GPUs
+/// (phys_share_chunk).
+pub fn share_chunk(n: usize, world: i32) -> usize {
+    let c = unsafe { ffi::phys_share_chunk(n as i64, world) };
+    if c < 0 { 0 } else { c as usize }
+}
+
 pub fn status_string(st: i32) -> String {
     unsafe { CStr::from_ptr(ffi::phys_status_string(st)) }.to_string_lossy().into_owned()
 }
