@@ -323,6 +323,18 @@ impl PhysGpu {
         Ok(a)
     }
 
+    /// velocity_verlet_position_system on the device state
+    /// (PreviousAcceleration = Acceleration; x += v dt + a dt^2/2).
+    pub fn vv_position_step(&mut self, dt: f64) -> Result<()> {
+        self.check(unsafe { ffi::phys_vv_position_step(self.raw(), dt) })
+    }
+
+    /// velocity_verlet_velocity_system on the device state
+    /// (v += (PreviousAcceleration + Acceleration) dt/2).
+    pub fn vv_velocity_step(&mut self, dt: f64) -> Result<()> {
+        self.check(unsafe { ffi::phys_vv_velocity_step(self.raw(), dt) })
+    }
+
     /// Share `rank` of `world` of the acceleration evaluation
     /// (phys_gravity_accel_share) for one system held whole by every GPU,
     /// packed into `share_out`; the caller all-gathers the shares (NCCL)
