@@ -64,7 +64,12 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip FP64 comparison and accuracy")
     ap.add_argument("--quick", action="store_true",
                     help="device-resident timing only (no e2e, extras, CPU baseline): profiling")
+    ap.add_argument("--precision", default="f32c", choices=["f32c", "f64", "f64_exact"],
+                    help="with --quick: the precision of the timed Barnes-Hut steps (the full "
+                         "line always times F32C, the metric's form)")
     a = ap.parse_args()
+    if a.precision != "f32c" and not a.quick:
+        ap.error("--precision other than f32c needs --quick")
     defaults = {  # n, theta, eps, dt per workload shape
         "bh": (1 << 20, 0.5, 0.01, 1e-3), "galaxy": (1 << 24, 0.6, 0.02, 5e-4),
         "bh_shared": (1 << 20, 0.5, 0.01, 1e-3),
@@ -255,10 +260,10 @@ def workload_config(args, precision, leaf_cap, walk="body"):
 # DRAM bytes (read + write) of one launch of the dominant kernel for the
 # default workload (N = 2^20 Plummer, theta 0.5, leaf capacity 8, F32C), each
 # from one ncu capture of this binary at full size:
-#   group walk, geval_kernel<true>: dram__bytes_read.sum 472.2 MB +
-#     dram__bytes_write.sum 53.5 MB;
+#   group walk, geval_kernel<true>: dram__bytes_read.sum 471.8 MB +
+#     dram__bytes_write.sum 52.1 MB;
 #   per-body walk, walk2_kernel: 131.8 MB + 25.3 MB.
-WALK_TRAFFIC_BYTES = {"group": 525.69e6, "body": 157.05e6}
+WALK_TRAFFIC_BYTES = {"group": 523.97e6, "body": 157.05e6}
 
 
 def walk_traffic(args):
@@ -292,6 +297,9 @@ def run_ours(args, ws, rank, local):
     n = args.n
     flags = physgpu.GROUP_WALK if args.walk == "group" else 0
     p32 = make_params(1.0, args.eps, args.theta, BARNES_HUT, F32C, args.leaf_cap, flags)
+    p_timed = p32 if args.precision == "f32c" else make_params(
+        1.0, args.eps, args.theta, BARNES_HUT, physgpu.PRECISIONS[args.precision],
+        args.leaf_cap, flags)
     p64 = make_params(1.0, args.eps, args.theta, BARNES_HUT, F64, args.leaf_cap, flags)
 
     def barrier():
@@ -325,12 +333,12 @@ def run_ours(args, ws, rank, local):
     eval_ms, eval_inter = [], []  # group walk: list-evaluation kernel (per timed step)
     ctx.upload(pos, vel, m)
     for _ in range(args.warmup):
-        ctx.verlet_steps(p32, args.dt, 1)
+        ctx.verlet_steps(p_timed, args.dt, 1)
     launches0 = ctx.timings()["launches"]
     clocks = Clocks(local)
     clocks.start()
     barrier()
-    tot_ms, walk_ms, inter = timed_steps(p32, args.steps)
+    tot_ms, walk_ms, inter = timed_steps(p_timed, args.steps)
     geval_ms, geval_inter = list(eval_ms), list(eval_inter)
     barrier()
     clk = clocks.stop()
@@ -368,11 +376,12 @@ def run_ours(args, ws, rank, local):
     d2h = n * 8 * 9
 
     def e2e_step():
-        st = lib.phys_state_upload(ctx.h, n, *[ptr(a) for a in X], *[ptr(a) for a in V], ptr(M))
-        st = st or lib.phys_state_set_accel(ctx.h, *[ptr(a) for a in A])
-        st = st or lib.phys_verlet_steps(ctx.h, ctypes.byref(p32), args.dt, 1)
-        st = st or lib.phys_state_download(ctx.h, *[ptr(a) for a in X], *[ptr(a) for a in V],
-                                           *[ptr(a) for a in A])
+        # one tick on host state in one call: upload of x, v, m and the
+        # Acceleration component, the tick, x, v, a back in place (the
+        # positions' copy back overlaps the force pass: page-locked arrays)
+        st = lib.phys_verlet_tick_host(ctx.h, ctypes.byref(p32), args.dt, n,
+                                       *[ptr(a) for a in X], *[ptr(a) for a in V], ptr(M),
+                                       *[ptr(a) for a in A])
         if st:
             raise physgpu.PhysError(st, lib.phys_last_error(ctx.h).decode())
 
@@ -510,7 +519,8 @@ def run_ours(args, ws, rank, local):
             "config": workload_config(args, "f32c (f32 pair terms, two-sum, f64 state)",
                                       args.leaf_cap, args.walk),
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "call": "phys_verlet_tick_host (page-locked "
+                    "host arrays; x, v, m, a in, x, v, a back)"},
             "gpu_launches": launches, "clocks": clk, "roofline": roof, "cpu_baseline": cpu,
             "interactions_per_step": inter_med, "nodes": tm["nodes"], "tree_depth_max": tm["max_depth"],
         }

@@ -271,6 +271,15 @@ int phys_vv_velocity_step(phys_ctx* ctx, double dt);
 /* As phys_verlet_steps but returns once the work is enqueued on the
  * context's stream (host sync only for the BH node count). */
 int phys_verlet_steps_async(phys_ctx* ctx, const phys_params* p, double dt, int64_t nsteps);
+/* One tick on host state in one call, the work of phys_state_upload +
+ * phys_state_set_accel (a: the Acceleration component, PreviousAcceleration
+ * of the position step) + phys_verlet_steps(1) + phys_state_download,
+ * results in place (x, v, a; m is read only).  When x, y, z are page-locked
+ * (cudaHostAlloc / cudaHostRegister) their copy back runs while the force
+ * pass computes.  Synchronous at return. */
+int phys_verlet_tick_host(phys_ctx* ctx, const phys_params* p, double dt, int64_t n, double* x,
+                          double* y, double* z, double* vx, double* vy, double* vz,
+                          const double* m, double* ax, double* ay, double* az);
 
 /* ---- batched ensemble of independent small systems ------------------- */
 /* Thousands of independent systems (1..64 bodies each) in CSR layout:

@@ -50,6 +50,11 @@ struct phys_ctx {
   // forks from and joins back into `stream` within one library call
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  // copy stream of phys_verlet_tick_host: the positions go back to the host
+  // while the force pass runs (copy_x: page-locked host arrays, or null)
+  cudaStream_t copy = nullptr;
+  cudaEvent_t copy_fork = nullptr, copy_done = nullptr;
+  double* copy_x[3] = {nullptr, nullptr, nullptr};
   std::string err;
   uint64_t launches = 0;
   phys_timings tm{};
@@ -109,6 +114,21 @@ struct phys_ctx {
   // Bound on one look-back wait of the radix sort, in re-reads of a tile's
   // status word (see sort.cu); phys_debug_set_wait_limit lowers it in tests.
   int64_t sort_spin_limit = int64_t(1) << 20;
+
+  // ---- CUDA graph of one direct-sum tick (force pass + fused velocity and
+  // position steps), replayed for the middle ticks of phys_verlet_steps; kept
+  // while what it was captured with is unchanged (ws_gen counts every move
+  // of a device buffer: a workspace slot or the state arrays) ----
+  cudaGraphExec_t tick_exec = nullptr;
+  uint64_t tick_launches = 0;  // kernel launches in one replay
+  phys_params tick_params{};
+  double tick_dt = 0.0;
+  int64_t tick_n = -1;
+  bool tick_halo_on = false;
+  phys_nfw_halo tick_halo{};
+  uint64_t tick_gen = ~uint64_t(0);
+  uint64_t ws_gen = 0;
+  bool capturing = false;  // enqueueing into a capture: no timing events
 
   // ---- small device scalars ----
   int32_t* d_status = nullptr;               // kStat* bits

@@ -49,6 +49,7 @@ void* ws_get(phys_ctx* c, int slot, size_t bytes, int* status) {
   }
   size_t want = bytes + bytes / 8;  // headroom for slowly growing sizes
   want = (want + 255) & ~size_t(255);
+  ++c->ws_gen;
   cudaError_t e = cudaMalloc(&b.p, want);
   if (e != cudaSuccess) {
     b.p = nullptr;
@@ -117,6 +118,7 @@ int ensure_state(phys_ctx* c, int64_t n) {
   }
   int64_t cap = n < 1024 ? 1024 : n;
   double* base = nullptr;
+  ++c->ws_gen;
   cudaError_t e = cudaMalloc(&base, sizeof(double) * 16 * size_t(cap));
   if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc(state)");
   double** slots[16] = {&c->x,  &c->y,  &c->z,  &c->vx,  &c->vy,  &c->vz,  &c->m,  &c->ax,
@@ -279,6 +281,60 @@ int verlet_steps_sectors(phys_ctx* c, const phys_params* p, double dt, int64_t n
   return PHYS_OK;
 }
 
+static bool same_halo(const phys_nfw_halo& a, const phys_nfw_halo& b) {
+  return a.rho_0 == b.rho_0 && a.scale_radius == b.scale_radius && a.center[0] == b.center[0] &&
+         a.center[1] == b.center[1] && a.center[2] == b.center[2] && a.enabled == b.enabled;
+}
+
+// The graph of one direct-sum tick body (force pass at x, then the velocity
+// step fused with the next position step), captured once and kept while n,
+// the parameters, dt, the halo and every device buffer are the same.  Its
+// kernels are the ones the loop would launch, so a replay is bit-identical
+// to them.  Returns false (nothing captured, nothing left pending) when the
+// capture fails; the caller then launches the tick itself.
+static bool tick_graph(phys_ctx* c, const phys_params* p, double dt) {
+  if (c->tick_exec && c->tick_n == c->n && same_params(c->tick_params, *p) && c->tick_dt == dt &&
+      c->tick_halo_on == c->halo_on && (!c->halo_on || same_halo(c->tick_halo, c->halo)) &&
+      c->tick_gen == c->ws_gen)
+    return true;
+  if (c->tick_exec) {
+    cudaGraphExecDestroy(c->tick_exec);
+    c->tick_exec = nullptr;
+  }
+  if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  const uint64_t gen0 = c->ws_gen, l0 = c->launches;
+  c->capturing = true;
+  int st = eval(c, p, false);
+  if (st == PHYS_OK) st = verlet_kick_drift(c, dt);
+  c->capturing = false;
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  cudaGraphExec_t exec = nullptr;
+  const bool ok = st == PHYS_OK && e == cudaSuccess && g && c->ws_gen == gen0 &&
+                  cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();
+  const uint64_t nl = c->launches - l0;  // counted as they are replayed
+  c->launches = l0;
+  if (!ok) {
+    if (exec) cudaGraphExecDestroy(exec);
+    c->err.clear();
+    return false;
+  }
+  c->tick_exec = exec;
+  c->tick_launches = nl;
+  c->tick_n = c->n;
+  c->tick_params = *p;
+  c->tick_dt = dt;
+  c->tick_halo_on = c->halo_on;
+  c->tick_halo = c->halo;
+  c->tick_gen = c->ws_gen;
+  return true;
+}
+
 int verlet_steps(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, bool sync) {
   PHYS_TRY(check_params(c, p));
   if (nsteps < 0) return fail(c, PHYS_ERR_ARG, "nsteps < 0");
@@ -294,8 +350,30 @@ int verlet_steps(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, b
     c->accel_valid = true;
   }
   c->accel_params = *p;
+  // the direct sum's ticks have no host synchronisation: the middle ones
+  // replay a captured graph of one tick (one launch instead of a handful)
+  const bool by_graph = p->method == PHYS_DIRECT && nsteps >= 4 && !c->copy_x[0];
   for (int64_t s = 0; s < nsteps; ++s) {
-    if (s == 0) PHYS_TRY(verlet_drift(c, dt));
+    if (by_graph && s == 1 && tick_graph(c, p, dt)) {
+      // ticks 1 .. nsteps-2: force pass, velocity step, next position step
+      for (; s + 1 < nsteps; ++s) {
+        PHYS_CUDA(c, cudaGraphLaunch(c->tick_exec, c->stream));
+        c->launches += c->tick_launches;
+      }
+    }
+    if (s == 0) {
+      PHYS_TRY(verlet_drift(c, dt));
+      if (nsteps == 1 && c->copy_x[0]) {
+        // the tick's positions are final: copy them back beside the force pass
+        PHYS_CUDA(c, cudaEventRecord(c->copy_fork, c->stream));
+        PHYS_CUDA(c, cudaStreamWaitEvent(c->copy, c->copy_fork, 0));
+        const double* src[3] = {c->x, c->y, c->z};
+        for (int k = 0; k < 3; ++k)
+          PHYS_CUDA(c, cudaMemcpyAsync(c->copy_x[k], src[k], sizeof(double) * c->n,
+                                       cudaMemcpyDeviceToHost, c->copy));
+        PHYS_CUDA(c, cudaEventRecord(c->copy_done, c->copy));
+      }
+    }
     c->accel_valid = false;
     PHYS_TRY(eval(c, p, false));  // chain 2 force pass at x_{n+1}
     c->accel_valid = true;
@@ -363,6 +441,12 @@ int phys_ctx_create(int device, phys_ctx** out) {
       st = cuda_fail(c, e, "cudaEventCreate(fork/join)");
       break;
     }
+    if ((e = cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->copy_fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->copy_done, cudaEventDisableTiming)) != cudaSuccess) {
+      st = cuda_fail(c, e, "cudaStreamCreate(copy)");
+      break;
+    }
     char* small = nullptr;
     if ((e = cudaMalloc(&small, 4096)) != cudaSuccess) { st = cuda_fail(c, e, "cudaMalloc(small)"); break; }
     c->d_status = reinterpret_cast<int32_t*>(small);
@@ -389,6 +473,7 @@ int phys_ctx_destroy(phys_ctx* c) {
   if (!c) return PHYS_OK;
   cudaSetDevice(c->device);
   if (c->side) cudaStreamSynchronize(c->side);
+  if (c->copy) cudaStreamSynchronize(c->copy);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (auto& b : c->ws)
     if (b.p) cudaFree(b.p);
@@ -403,6 +488,10 @@ int phys_ctx_destroy(phys_ctx* c) {
   if (c->fork) cudaEventDestroy(c->fork);
   if (c->join) cudaEventDestroy(c->join);
   if (c->side) cudaStreamDestroy(c->side);
+  if (c->copy_fork) cudaEventDestroy(c->copy_fork);
+  if (c->copy_done) cudaEventDestroy(c->copy_done);
+  if (c->copy) cudaStreamDestroy(c->copy);
+  if (c->tick_exec) cudaGraphExecDestroy(c->tick_exec);
   if (c->stream) cudaStreamDestroy(c->stream);
   cudaGetLastError();
   delete c;
@@ -837,6 +926,61 @@ int phys_direct_accel_targets(phys_ctx* c, const phys_params* p, int64_t nt,
 int phys_verlet_steps(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps) {
   PHYS_ENTER(c);
   return verlet_steps(c, p, dt, nsteps, true);
+}
+
+// Whether every pointer is page-locked host memory (an asynchronous copy
+// from it does not wait for the host).
+static bool all_pinned(const double* const* a, int k) {
+  for (int i = 0; i < k; ++i) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, a[i]) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    if (at.type != cudaMemoryTypeHost) return false;
+  }
+  return true;
+}
+
+int phys_verlet_tick_host(phys_ctx* c, const phys_params* p, double dt, int64_t n, double* x,
+                          double* y, double* z, double* vx, double* vy, double* vz,
+                          const double* m, double* ax, double* ay, double* az) {
+  PHYS_ENTER(c);
+  if (!x || !y || !z || !vx || !vy || !vz || !m || !ax || !ay || !az)
+    return fail(c, PHYS_ERR_ARG, "every state array is required");
+  PHYS_TRY(phys_state_upload(c, n, x, y, z, vx, vy, vz, m));
+  if (n == 0) return PHYS_OK;
+  PHYS_TRY(h2d(c, c->ax, ax, n));
+  PHYS_TRY(h2d(c, c->ay, ay, n));
+  PHYS_TRY(h2d(c, c->az, az, n));
+  c->accel_valid = true;
+  c->accel_params.method = -1;  // the caller's Acceleration component
+  const double* xs[3] = {x, y, z};
+  const bool early = all_pinned(xs, 3);
+  if (early) {
+    c->copy_x[0] = x;
+    c->copy_x[1] = y;
+    c->copy_x[2] = z;
+  }
+  const int st_run = verlet_steps(c, p, dt, 1, false);
+  c->copy_x[0] = c->copy_x[1] = c->copy_x[2] = nullptr;
+  if (early) PHYS_CUDA(c, cudaStreamWaitEvent(c->stream, c->copy_done, 0));
+  PHYS_TRY(st_run);
+  if (!early) {
+    PHYS_TRY(d2h(c, x, c->x, n));
+    PHYS_TRY(d2h(c, y, c->y, n));
+    PHYS_TRY(d2h(c, z, c->z, n));
+  }
+  PHYS_TRY(d2h(c, vx, c->vx, n));
+  PHYS_TRY(d2h(c, vy, c->vy, n));
+  PHYS_TRY(d2h(c, vz, c->vz, n));
+  PHYS_TRY(d2h(c, ax, c->ax, n));
+  PHYS_TRY(d2h(c, ay, c->ay, n));
+  PHYS_TRY(d2h(c, az, c->az, n));
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int st = finish_status(c);
+  c->tm.total_ms = ev_ms(c->ev[0], c->ev[1]);
+  return st;
 }
 
 int phys_verlet_steps_async(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps) {

@@ -14,49 +14,90 @@ namespace {
 // F64_EXACT: the reference's arithmetic, j in order 0..N-1, no FMA.
 //   r = x_j - x_i; r2 = len2(r); s2 = r2 + eps2; s3 = s2 * sqrt(s2)
 //   sc = ((G*m_i)*m_j)/s3; F += r*sc            (gravity.rs:58-65)
-// One thread per target; the j order fixes the summation, so no slicing.
+// Only the additions into F are ordered; the terms r*sc are independent.  A
+// block takes kXT targets: in round k its compute warps evaluate the terms
+// of sources [k kXJ, (k+1) kXJ) against every target into shared memory
+// (each thread one source against two targets, the source of round k+1
+// loaded ahead), while lane t of warp 0 adds round k-1's terms of target t
+// in j order, skipping j == i as the reference does.  The divides and square
+// roots, whose latency bounded the one-thread-per-target form, run in
+// parallel; the sum is the reference's bit for bit.
 // ---------------------------------------------------------------------------
-constexpr int kExactBlock = 64;
+constexpr int kXT = 8;                    // targets per block
+constexpr int kXJ = 64;                   // sources per round
+constexpr int kXCompute = kXT * kXJ / 2;  // compute threads: two targets each
+constexpr int kXBlock = 32 + kXCompute;   // warp 0 adds, the rest compute
+static_assert(kXT <= 32 && kXCompute % 32 == 0 && kXJ % 32 == 0, "exact block layout");
 
-__global__ void __launch_bounds__(kExactBlock)
+__global__ void __launch_bounds__(kXBlock)
 direct_exact_kernel(int64_t n, int64_t t0, int64_t t1, const double* __restrict__ x,
                     const double* __restrict__ y, const double* __restrict__ z,
                     const double* __restrict__ m, double G, double eps2, int want_force,
                     double* __restrict__ ox, double* __restrict__ oy, double* __restrict__ oz,
                     int32_t* status) {
-  __shared__ double4 tile[kExactBlock];
-  const int64_t i = t0 + blockIdx.x * (int64_t)kExactBlock + threadIdx.x;
-  const bool valid = i < t1;
-  double xi = 0, yi = 0, zi = 0, mi = 0;
-  if (valid) {
-    xi = x[i];
-    yi = y[i];
-    zi = z[i];
-    mi = m[i];
+  __shared__ double term[2][3][kXT][kXJ + 1];  // [round parity][x, y, z][target][source]
+  __shared__ double4 tgt[kXT];                 // x_i, y_i, z_i, G*m_i
+  const int tid = threadIdx.x;
+  const int64_t i0 = t0 + blockIdx.x * (int64_t)kXT;
+  if (tid < kXT) {
+    const int64_t i = i0 + tid;
+    tgt[tid] = i < t1 ? make_double4(x[i], y[i], z[i], xmul(G, m[i]))
+                      : make_double4(0.0, 0.0, 0.0, 0.0);
   }
-  const double gm = xmul(G, mi);
-  double fx = 0.0, fy = 0.0, fz = 0.0;
-  for (int64_t base = 0; base < n; base += kExactBlock) {
-    int64_t j = base + threadIdx.x;
-    __syncthreads();
-    tile[threadIdx.x] = j < n ? make_double4(x[j], y[j], z[j], m[j]) : make_double4(0, 0, 0, 0);
-    __syncthreads();
-    const int cnt = (int)min64(kExactBlock, n - base);
-    for (int k = 0; k < cnt; ++k) {
-      if (base + k == i) continue;
-      const double4 s = tile[k];
-      const double rx = xsub(s.x, xi), ry = xsub(s.y, yi), rz = xsub(s.z, zi);
-      const double r2 = xlen2(rx, ry, rz);
-      const double s2 = xadd(r2, eps2);
-      const double s3 = xmul(s2, xsqrt(s2));
-      const double sc = xdiv(xmul(gm, s.w), s3);
-      fx = xadd(fx, xmul(rx, sc));
-      fy = xadd(fy, xmul(ry, sc));
-      fz = xadd(fz, xmul(rz, sc));
+  __syncthreads();
+  const int64_t rounds = ceil_div(n, kXJ);
+  // compute threads: source slot jj, targets ta and ta + kXT/2
+  const int c = tid - 32, jj = c % kXJ, ta = c / kXJ;
+  double4 src = make_double4(0.0, 0.0, 0.0, 0.0);
+  if (tid >= 32 && jj < n) src = make_double4(x[jj], y[jj], z[jj], m[jj]);
+  double fx = 0.0, fy = 0.0, fz = 0.0;  // warp 0, lane t < kXT: target t
+  for (int64_t k = 0; k <= rounds; ++k) {
+    const int b = (int)(k & 1);
+    if (tid >= 32) {
+      if (k < rounds) {
+        const int64_t j = k * kXJ + jj;
+        const int64_t jn = j + kXJ;
+        double4 next = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (jn < n) next = make_double4(x[jn], y[jn], z[jn], m[jn]);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int t = ta + h * (kXT / 2);
+          const double4 T = tgt[t];
+          double ax = 0.0, ay = 0.0, az = 0.0;
+          if (j < n && i0 + t < t1) {
+            const double rx = xsub(src.x, T.x), ry = xsub(src.y, T.y), rz = xsub(src.z, T.z);
+            const double s2 = xadd(xlen2(rx, ry, rz), eps2);
+            const double sc = xdiv(xmul(T.w, src.w), xmul(s2, xsqrt(s2)));
+            ax = xmul(rx, sc);
+            ay = xmul(ry, sc);
+            az = xmul(rz, sc);
+          }
+          term[b][0][t][jj] = ax;
+          term[b][1][t][jj] = ay;
+          term[b][2][t][jj] = az;
+        }
+        src = next;
+      }
+    } else if (k > 0 && tid < kXT) {
+      const int pb = b ^ 1;
+      const int64_t jb = (k - 1) * kXJ;
+      const int cnt = (int)min64(kXJ, n - jb);
+      const int64_t self = i0 + tid - jb;  // j == i sits at slot self, if in [0, cnt)
+      for (int q = 0; q < cnt; ++q) {
+        if (q == self) continue;
+        fx = xadd(fx, term[pb][0][tid][q]);
+        fy = xadd(fy, term[pb][1][tid][q]);
+        fz = xadd(fz, term[pb][2][tid][q]);
+      }
     }
+    __syncthreads();
   }
+  if (tid >= 32) return;
+  const int64_t i = i0 + tid;
+  const bool valid = tid < kXT && i < t1;
   if (valid) {
     if (!want_force) {  // compute_acceleration_system: a = F / m (integrators.rs:115)
+      const double mi = m[i];
       fx = xdiv(fx, mi);
       fy = xdiv(fy, mi);
       fz = xdiv(fz, mi);
@@ -66,7 +107,7 @@ direct_exact_kernel(int64_t n, int64_t t0, int64_t t1, const double* __restrict_
     oz[i] = fz;
   }
   bool bad = valid && (!isfinite(fx) || !isfinite(fy) || !isfinite(fz));
-  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(status, kStatNonfinite);
+  if (__any_sync(0xffffffffu, bad) && tid == 0) atomicOr(status, kStatNonfinite);
 }
 
 // ---------------------------------------------------------------------------
@@ -364,7 +405,7 @@ int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, 
   const int64_t n = c->n;
   const double eps2 = p->eps * p->eps;
   PHYS_CUDA(c, cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned long long), c->stream));
-  PHYS_CUDA(c, cudaEventRecord(c->ev[6], c->stream));
+  if (!c->capturing) PHYS_CUDA(c, cudaEventRecord(c->ev[6], c->stream));
   // targets [t0, t1): all, or the share (t0 a multiple of kTile); the slices
   // follow from n alone, so a target's sum does not depend on the share
   int64_t t0 = 0, t1 = n;
@@ -372,13 +413,13 @@ int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, 
   if (t0 % kTile) return fail(c, PHYS_ERR_ARG, "direct-sum share must start on a tile");
   const int64_t nt = t1 - t0;
   if (nt <= 0) {
-    PHYS_CUDA(c, cudaEventRecord(c->ev[7], c->stream));
+    if (!c->capturing) PHYS_CUDA(c, cudaEventRecord(c->ev[7], c->stream));
     c->tm.interactions = 0;
     return PHYS_OK;
   }
   if (p->precision == PHYS_F64_EXACT) {
-    PHYS_LAUNCH(c, direct_exact_kernel, (int)ceil_div(nt, kExactBlock), kExactBlock, 0, n, t0, t1,
-                c->x, c->y, c->z, c->m, p->G, eps2, (int)want_force, ox, oy, oz, c->d_status);
+    PHYS_LAUNCH(c, direct_exact_kernel, (int)ceil_div(nt, kXT), kXBlock, 0, n, t0, t1, c->x, c->y,
+                c->z, c->m, p->G, eps2, (int)want_force, ox, oy, oz, c->d_status);
   } else {
     const int64_t slices = choose_slices(n);
     const int64_t slice_len = ceil_div(ceil_div(n, slices), kTile) * kTile;
@@ -410,7 +451,7 @@ int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, 
                   (int)want_force, ox, oy, oz, c->d_status);
     }
   }
-  PHYS_CUDA(c, cudaEventRecord(c->ev[7], c->stream));
+  if (!c->capturing) PHYS_CUDA(c, cudaEventRecord(c->ev[7], c->stream));
   c->tm.interactions = (uint64_t)nt * (uint64_t)(n - 1);
   c->tm.bbox_ms = c->tm.keys_ms = c->tm.sort_ms = c->tm.tree_ms = 0.0;
   c->tm.nodes = 0;

@@ -168,12 +168,19 @@ radix_pass_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__
   const int64_t base = tile0 + warp * kWarpKeys;
   const unsigned lt = lanemask_lt();
   uint64_t key[kItems];
-  uint32_t rank[kItems];
+  uint32_t rank[kItems], val[kItems];
+  // every load of the tile first, so that they are in flight together: the
+  // ranking rounds below synchronise the warp, which loads may not cross
+#pragma unroll
+  for (int r = 0; r < kItems; ++r) {
+    const int64_t idx = base + r * 32 + lane;
+    key[r] = idx < n ? kin[idx] : 0ull;
+    if (kHasVals) val[r] = idx < n ? vin[idx] : 0u;
+  }
 #pragma unroll
   for (int r = 0; r < kItems; ++r) {
     const int64_t idx = base + r * 32 + lane;
     const bool v = idx < n;
-    key[r] = v ? kin[idx] : 0ull;
     const uint32_t d = (uint32_t)(key[r] >> shift) & 0xFFu;
     const unsigned act = __ballot_sync(0xffffffffu, v);
     const unsigned peers = match_digit(act, d);
@@ -275,7 +282,7 @@ radix_pass_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__
       const uint32_t d = (uint32_t)(key[r] >> shift) & 0xFFu;
       const uint32_t lpos = cnt[warp][d] + rank[r];
       skey[lpos] = key[r];
-      if (kHasVals) sval[lpos] = vin[idx];
+      if (kHasVals) sval[lpos] = val[r];
     }
   }
   __syncthreads();

@@ -252,12 +252,13 @@ __device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); 
 __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
 
 __global__ void __launch_bounds__(kWalk2Block)
-walk2_kernel(int q0, int n, int nnodes, const Rec32x2* __restrict__ w, const Body32x2* __restrict__ body2,
+walk2_kernel(int q64, int n, int nnodes, const Rec32x2* __restrict__ w, const Body32x2* __restrict__ body2,
              const double4* __restrict__ body64, const uint32_t* __restrict__ perm, double G,
              double eps2, int want_force, double* __restrict__ ox, double* __restrict__ oy,
              double* __restrict__ oz, unsigned long long* counter, int32_t* status) {
   const int lane = threadIdx.x & 31;
-  const int base = q0 + (blockIdx.x * (kWalk2Block / 32) + (threadIdx.x >> 5)) * 64;
+  // targets [64 q64, n), 64 per warp (a multiple of 64: pa even)
+  const int base = (q64 + blockIdx.x * (kWalk2Block / 32) + (threadIdx.x >> 5)) * 64;
   const int pa = base + 2 * lane, pb = pa + 1;
   const bool va = pa < n, vb = pb < n;
   float2 nhx, nhy, nhz, nlx, nly, nlz;  // negated target coordinates (a, b)
@@ -494,8 +495,9 @@ int bh_walk(phys_ctx* c, const phys_params* p, const BhTree& t, bool want_force,
                 t.body64, t.body_hi, t.body_lo, t.perm, t.hdr, p->G, eps2, (int)want_force, ox, oy,
                 oz, c->d_counter, c->d_status);
   } else if (WALK_PAIRED && t.w32x2) {
+    if (q0 % 64) return fail(c, PHYS_ERR_ARG, "per-body walk share must start at a multiple of 64");
     const int grid2 = (int)ceil_div(nt > 0 ? nt : 1, 64 * (kWalk2Block / 32));
-    PHYS_LAUNCH(c, walk2_kernel, grid2, kWalk2Block, 0, (int)q0, (int)q1, (int)t.nnodes, t.w32x2, t.body2,
+    PHYS_LAUNCH(c, walk2_kernel, grid2, kWalk2Block, 0, (int)(q0 / 64), (int)q1, (int)t.nnodes, t.w32x2, t.body2,
                 t.body64, t.perm, p->G, eps2, (int)want_force, ox, oy, oz, c->d_counter,
                 c->d_status);
   } else {

@@ -55,7 +55,7 @@ EXPORTED = [
     "phys_nfw_density", "phys_nfw_enclosed_mass", "phys_nfw_circular_velocity",
     "phys_nfw_forces", "phys_set_nfw_halo", "phys_state_upload_sector_state",
     "phys_state_download_sector_state", "phys_debug_set_wait_limit", "phys_share_chunk",
-    "phys_gravity_accel_share", "phys_gravity_accel_unshare",
+    "phys_gravity_accel_share", "phys_gravity_accel_unshare", "phys_verlet_tick_host",
 ]
 
 
@@ -156,6 +156,7 @@ def load_library(path=None):
         "phys_share_chunk": ([i64, i32], i64),
         "phys_gravity_accel_share": ([_VP, P, i32, i32, _VP], ctypes.c_int),
         "phys_gravity_accel_unshare": ([_VP, i32, _VP], ctypes.c_int),
+        "phys_verlet_tick_host": ([_VP, P, dbl, i64] + [_D] * 10, ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -440,6 +441,20 @@ class Context:
     def verlet_steps_async(self, params, dt, nsteps):
         self._check(self.lib.phys_verlet_steps_async(self.h, ctypes.byref(params), float(dt),
                                                      int(nsteps)), "phys_verlet_steps_async")
+
+    def verlet_tick_host(self, params, dt, x, v, m, a):
+        """One tick on host state in one call (phys_verlet_tick_host): x, v, a
+        are lists of three contiguous float64 arrays (numpy, or page-locked
+        torch tensors) updated in place; m is read."""
+        def ptr(t):
+            if hasattr(t, "data_ptr"):
+                return ctypes.cast(t.data_ptr(), _D)
+            return _p(t)
+        n = len(m)
+        self._check(self.lib.phys_verlet_tick_host(
+            self.h, ctypes.byref(params), float(dt), n, *[ptr(t) for t in x],
+            *[ptr(t) for t in v], ptr(m), *[ptr(t) for t in a]), "phys_verlet_tick_host")
+        self.n = n
 
     def vv_position_step(self, dt):
         self._check(self.lib.phys_vv_position_step(self.h, float(dt)), "phys_vv_position_step")

@@ -147,6 +147,10 @@ extern "C" {
     // ---- integration ----
     pub fn phys_verlet_steps(ctx: *mut phys_ctx, p: *const phys_params, dt: f64,
                              nsteps: i64) -> c_int;
+    pub fn phys_verlet_tick_host(ctx: *mut phys_ctx, p: *const phys_params, dt: f64, n: i64,
+                                 x: *mut f64, y: *mut f64, z: *mut f64, vx: *mut f64,
+                                 vy: *mut f64, vz: *mut f64, m: *const f64, ax: *mut f64,
+                                 ay: *mut f64, az: *mut f64) -> c_int;
     pub fn phys_vv_position_step(ctx: *mut phys_ctx, dt: f64) -> c_int;
     pub fn phys_vv_velocity_step(ctx: *mut phys_ctx, dt: f64) -> c_int;
     pub fn phys_verlet_steps_async(ctx: *mut phys_ctx, p: *const phys_params, dt: f64,

@@ -363,6 +363,24 @@ impl PhysGpu {
         self.check(unsafe { ffi::phys_verlet_steps(self.raw(), p, dt, nsteps) })
     }
 
+    /// One tick on host state in one call (phys_verlet_tick_host): position
+    /// step, force pass, velocity step; x, v and a updated in place.
+    pub fn verlet_tick_host(&mut self, p: &ffi::phys_params, dt: f64, x: &mut Soa3,
+                            v: &mut Soa3, m: &[f64], a: &mut Soa3) -> Result<()> {
+        let n = m.len();
+        x.check_len(n, "positions")?;
+        v.check_len(n, "velocities")?;
+        a.check_len(n, "accelerations")?;
+        self.check(unsafe {
+            ffi::phys_verlet_tick_host(self.raw(), p, dt, n as i64, x.x.as_mut_ptr(),
+                                       x.y.as_mut_ptr(), x.z.as_mut_ptr(), v.x.as_mut_ptr(),
+                                       v.y.as_mut_ptr(), v.z.as_mut_ptr(), m.as_ptr(),
+                                       a.x.as_mut_ptr(), a.y.as_mut_ptr(), a.z.as_mut_ptr())
+        })?;
+        self.n = n;
+        Ok(())
+    }
+
     /// nfw_gravity_system's halo in every later acceleration (None removes it).
     pub fn set_nfw_halo(&mut self, halo: Option<&ffi::phys_nfw_halo>) -> Result<()> {
         let h = halo.map_or(null(), |h| h as *const _);

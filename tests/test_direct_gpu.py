@@ -47,7 +47,7 @@ def test_kepler_orbit_period_mirror(ctx):
     assert f[1] == 0.0 and f[2] == 0.0
 
 
-@pytest.mark.parametrize("n", [2, 3, 5, 17, 31, 32, 33, 63, 64, 65, 127, 129, 300])
+@pytest.mark.parametrize("n", [2, 3, 5, 8, 9, 17, 31, 32, 33, 63, 64, 65, 127, 129, 300, 1031])
 def test_exact_small_n_bitexact(ctx, n):
     rng = np.random.default_rng(n)
     pos = rng.normal(0, 1, (n, 3))

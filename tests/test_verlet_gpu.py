@@ -134,3 +134,30 @@ def test_energy_mirror_skips_coincident_pairs(ctx):
     assert ke == 0.5 * 2.0 * 1.0 + 0.5 * 1.0 * 4.0
     assert abs(pe - (-(2.0 / 5.0) - (3.0 / 5.0))) < 1e-15
     assert np.allclose(p, [2.0, 2.0, 0.0])
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_tick_host_equals_four_calls(ctx, pinned):
+    """phys_verlet_tick_host == upload + set_accel + one tick + download, bit
+    for bit, with pageable (numpy) and page-locked (torch) host arrays."""
+    import torch
+    n = 30000
+    pos, vel, m = ics.plummer(n, seed=6)
+    acc = np.random.default_rng(6).normal(size=(n, 3)) * 1e-3
+    p = make_params(1.0, 0.01, 0.5, physgpu.BARNES_HUT, physgpu.F32C, 8, physgpu.GROUP_WALK)
+    ctx.upload(pos, vel, m)
+    ctx.set_accel(acc)
+    ctx.verlet_steps(p, 1e-3, 1)
+    want = ctx.download()
+
+    def arrays(a):
+        cols = [np.ascontiguousarray(a[:, k]) for k in range(3)]
+        if not pinned:
+            return cols
+        return [torch.from_numpy(c).pin_memory() for c in cols]
+    X, V, A = arrays(pos), arrays(vel), arrays(acc)
+    M = torch.from_numpy(m.copy()).pin_memory() if pinned else m.copy()
+    ctx.verlet_tick_host(p, 1e-3, X, V, M, A)
+    got = [np.stack([np.asarray(c) for c in t], axis=1) for t in (X, V, A)]
+    for g, w in zip(got, want):
+        assert np.array_equal(g, w)
