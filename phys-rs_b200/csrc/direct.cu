@@ -21,7 +21,9 @@ namespace {
 // loaded ahead), while lane t of warp 0 adds round k-1's terms of target t
 // in j order, skipping j == i as the reference does.  The divides and square
 // roots, whose latency bounded the one-thread-per-target form, run in
-// parallel; the sum is the reference's bit for bit.
+// parallel; the sum is the reference's bit for bit.  What is left is the
+// ordered chain of N dependent f64 additions per component, the bound of
+// any exact form (1024 bodies: about 20 us per evaluation).
 // ---------------------------------------------------------------------------
 constexpr int kXT = 8;                    // targets per block
 constexpr int kXJ = 64;                   // sources per round
@@ -82,12 +84,25 @@ direct_exact_kernel(int64_t n, int64_t t0, int64_t t1, const double* __restrict_
       const int pb = b ^ 1;
       const int64_t jb = (k - 1) * kXJ;
       const int cnt = (int)min64(kXJ, n - jb);
-      const int64_t self = i0 + tid - jb;  // j == i sits at slot self, if in [0, cnt)
-      for (int q = 0; q < cnt; ++q) {
-        if (q == self) continue;
-        fx = xadd(fx, term[pb][0][tid][q]);
-        fy = xadd(fy, term[pb][1][tid][q]);
-        fz = xadd(fz, term[pb][2][tid][q]);
+      // j == i sits at slot self, if in [0, cnt): the slots before and after
+      // it as two straight runs, so that the loads run ahead of the adds
+      const int64_t self = i0 + tid - jb;
+      const int q1 = (int)(self < 0 ? 0 : self < cnt ? self : cnt);
+      const int q2 = self >= 0 && self < cnt ? q1 + 1 : q1;
+      const double* tx = term[pb][0][tid];
+      const double* ty = term[pb][1][tid];
+      const double* tz = term[pb][2][tid];
+#pragma unroll 16
+      for (int q = 0; q < q1; ++q) {
+        fx = xadd(fx, tx[q]);
+        fy = xadd(fy, ty[q]);
+        fz = xadd(fz, tz[q]);
+      }
+#pragma unroll 16
+      for (int q = q2; q < cnt; ++q) {
+        fx = xadd(fx, tx[q]);
+        fy = xadd(fy, ty[q]);
+        fz = xadd(fz, tz[q]);
       }
     }
     __syncthreads();
