@@ -10,8 +10,9 @@
  *
  * Conventions
  *  - Plain pointers and sizes; arrays are structure-of-arrays, f64, length n,
- *    in the caller's (ECS query) order.  Host pointers unless the name says
- *    "_device".
+ *    in the caller's (ECS query) order.  Host pointers, except the DEVICE
+ *    buffers of phys_direct_accel_noalloc and of the target-share calls
+ *    (phys_gravity_accel_share / _unshare), as their comments say.
  *  - Every call returns a status (PHYS_OK == 0).  No call aborts, throws or
  *    traps; on error phys_last_error() describes it.
  *  - A context owns its CUDA streams (a main stream, and a second one that
@@ -374,7 +375,8 @@ int phys_bh_export(phys_ctx* ctx, const phys_params* p, int64_t cap, int64_t* nn
  * process that calls cudaDeviceReset on a device must not call this entry
  * point on that device again.  All calls share the array, so calls that
  * overlap on the GPU race: order them.  n outside 0..32768 returns PHYS_ERR_ARG with a
- * message in errbuf (optional, errlen bytes).  Synchronous at return. */
+ * message in errbuf (optional, errlen bytes).  Synchronous at return (it
+ * reads its status word back), so no call can be captured in a CUDA graph. */
 int phys_direct_accel_noalloc(int64_t n, const double* x, const double* y, const double* z,
                               const double* m, double G, double eps, int32_t precision,
                               double* ax, double* ay, double* az, void* stream, char* errbuf,
