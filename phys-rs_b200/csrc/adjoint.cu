@@ -263,6 +263,69 @@ int copy_d2d(phys_ctx* c, double* dst, const double* src, int64_t count) {
   return PHYS_OK;
 }
 
+// A segment's launches are the same for every segment of the same length
+// (same kernels, same buffers: the forward steps, their recomputation, the
+// reverse steps), so each kind is captured in a CUDA graph once per length
+// and replayed: one launch per segment instead of several per step, and the
+// same kernels in the same order, so the results are the same bit for bit.
+// Segments whose host-side state does not return to its start (an odd
+// number of steps swaps a.A and a.A2) are launched directly.
+struct Replay {
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  int64_t len[2] = {-1, -1};  // segment length captured in each slot
+  uint64_t launches[2] = {0, 0};
+  Replay() = default;
+  Replay(const Replay&) = delete;
+  Replay& operator=(const Replay&) = delete;
+  ~Replay() {
+    for (cudaGraphExec_t e : exec)
+      if (e) cudaGraphExecDestroy(e);
+  }
+};
+
+template <class F>
+int run_segment(phys_ctx* c, Replay& R, int64_t len, bool replayable, F&& enqueue) {
+  int slot = R.len[0] == len ? 0 : (R.len[1] == len ? 1 : -1);
+  if (replayable && slot < 0) {
+    slot = R.exec[0] ? 1 : 0;
+    if (R.exec[slot]) {
+      cudaGraphExecDestroy(R.exec[slot]);
+      R.exec[slot] = nullptr;
+      R.len[slot] = -1;
+    }
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      const uint64_t l0 = c->launches;
+      const int st = enqueue();
+      cudaGraph_t g = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+      cudaGraphExec_t exec = nullptr;
+      const bool ok = st == PHYS_OK && e == cudaSuccess && g &&
+                      cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
+      if (g) cudaGraphDestroy(g);
+      R.launches[slot] = c->launches - l0;
+      c->launches = l0;
+      if (ok) {
+        R.exec[slot] = exec;
+        R.len[slot] = len;
+      } else {
+        // nothing ran: the segment is launched directly below (the
+        // capture's host-side state changes were a whole even segment)
+        if (exec) cudaGraphExecDestroy(exec);
+        cudaGetLastError();
+        c->err.clear();
+        slot = -1;
+      }
+    } else {
+      cudaGetLastError();
+      slot = -1;
+    }
+  }
+  if (!replayable || slot < 0) return enqueue();
+  PHYS_CUDA(c, cudaGraphLaunch(R.exec[slot], c->stream));
+  c->launches += R.launches[slot];
+  return PHYS_OK;
+}
+
 // x0, v0 of the context state into a.X, a.V (SoA blocks of 3n).
 int load_initial(phys_ctx* c, Adj& a) {
   const int64_t n = a.n;
@@ -275,16 +338,27 @@ int load_initial(phys_ctx* c, Adj& a) {
   return PHYS_OK;
 }
 
-int forward(phys_ctx* c, const phys_params* p, Adj& a, double dt, bool keep_ckpt) {
+int forward(phys_ctx* c, const phys_params* p, Adj& a, double dt, bool keep_ckpt,
+            Replay* R = nullptr) {
   PHYS_TRY(load_initial(c, a));
   PHYS_TRY(force(c, p, a, a.X, a.A));
-  for (int64_t k = 0; k < a.T; ++k) {
-    if (keep_ckpt && k % a.K == 0) {
-      double* ck = a.ckpt + (k / a.K) * 6 * a.n;
-      PHYS_TRY(copy_d2d(c, ck, a.X, 3 * a.n));
-      PHYS_TRY(copy_d2d(c, ck + 3 * a.n, a.V, 3 * a.n));
-    }
-    PHYS_TRY(step(c, p, a, dt));
+  if (!keep_ckpt) {
+    for (int64_t k = 0; k < a.T; ++k) PHYS_TRY(step(c, p, a, dt));
+    return PHYS_OK;
+  }
+  for (int64_t k0 = 0; k0 < a.T; k0 += a.K) {
+    double* ck = a.ckpt + (k0 / a.K) * 6 * a.n;
+    PHYS_TRY(copy_d2d(c, ck, a.X, 3 * a.n));
+    PHYS_TRY(copy_d2d(c, ck + 3 * a.n, a.V, 3 * a.n));
+    const int64_t len = std::min<int64_t>(a.K, a.T - k0);
+    auto steps = [&]() -> int {
+      for (int64_t j = 0; j < len; ++j) PHYS_TRY(step(c, p, a, dt));
+      return PHYS_OK;
+    };
+    if (R)
+      PHYS_TRY(run_segment(c, *R, len, len % 2 == 0, steps));
+    else
+      PHYS_TRY(steps());
   }
   return PHYS_OK;
 }
@@ -347,7 +421,8 @@ int adjoint(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, int64_
   PHYS_TRY(setup(c, nsteps, K, true, a));
   const int64_t n = a.n;
   PHYS_TRY(upload_targets(c, a, tx, ty, tz));
-  PHYS_TRY(forward(c, p, a, dt, true));
+  Replay fwd, rec, rev;  // captured segments: forward, recomputation, reverse
+  PHYS_TRY(forward(c, p, a, dt, true, &fwd));
   double l = 0.0;
   PHYS_TRY(loss_of(c, a, true, &l));  // xbar = dL/dx_T
   PHYS_CUDA(c, cudaMemsetAsync(a.vbar, 0, sizeof(double) * 3 * n, c->stream));
@@ -361,17 +436,25 @@ int adjoint(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, int64_
     const double* ck = a.ckpt + s * 6 * n;
     PHYS_TRY(copy_d2d(c, a.X, ck, 3 * n));
     PHYS_TRY(copy_d2d(c, a.V, ck + 3 * n, 3 * n));
-    PHYS_TRY(force(c, p, a, a.X, a.A));
-    PHYS_TRY(copy_d2d(c, a.seg, a.X, 3 * n));
-    for (int64_t j = 0; j < len; ++j) {
-      PHYS_TRY(step(c, p, a, dt));
-      PHYS_TRY(copy_d2d(c, a.seg + (j + 1) * 3 * n, a.X, 3 * n));
-    }
-    for (int64_t j = len - 1; j >= 0; --j) {  // reverse of step k = k0 + j
-      PHYS_LAUNCH(c, adj_pre, grid_for(3 * n), kBlock, 0, n, h, a.abar, a.vbar);
-      PHYS_TRY(vjp(c, p, a, a.seg + (j + 1) * 3 * n));
-      PHYS_LAUNCH(c, adj_post, grid_for(3 * n), kBlock, 0, n, dt, a.abar, a.vbar, a.xbar);
-    }
+    auto recompute = [&]() -> int {
+      PHYS_TRY(force(c, p, a, a.X, a.A));
+      PHYS_TRY(copy_d2d(c, a.seg, a.X, 3 * n));
+      for (int64_t j = 0; j < len; ++j) {
+        PHYS_TRY(step(c, p, a, dt));
+        PHYS_TRY(copy_d2d(c, a.seg + (j + 1) * 3 * n, a.X, 3 * n));
+      }
+      return PHYS_OK;
+    };
+    PHYS_TRY(run_segment(c, rec, len, len % 2 == 0, recompute));
+    auto reverse = [&]() -> int {
+      for (int64_t j = len - 1; j >= 0; --j) {  // reverse of step k = k0 + j
+        PHYS_LAUNCH(c, adj_pre, grid_for(3 * n), kBlock, 0, n, h, a.abar, a.vbar);
+        PHYS_TRY(vjp(c, p, a, a.seg + (j + 1) * 3 * n));
+        PHYS_LAUNCH(c, adj_post, grid_for(3 * n), kBlock, 0, n, dt, a.abar, a.vbar, a.xbar);
+      }
+      return PHYS_OK;
+    };
+    PHYS_TRY(run_segment(c, rev, len, true, reverse));
   }
   // a_0 = A(x_0)
   PHYS_TRY(load_initial(c, a));
