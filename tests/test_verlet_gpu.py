@@ -161,3 +161,27 @@ def test_tick_host_equals_four_calls(ctx, pinned):
     got = [np.stack([np.asarray(c) for c in t], axis=1) for t in (X, V, A)]
     for g, w in zip(got, want):
         assert np.array_equal(g, w)
+
+
+@pytest.mark.parametrize("prec", [F64_EXACT, F64, F32C])
+def test_graph_replayed_ticks_equal_single_ticks(ctx, prec):
+    """The direct sum's middle ticks replay a captured graph: a 7-tick run
+    equals seven 1-tick runs bit for bit, and the cached graph follows a
+    change of dt, of the parameters and of the body count."""
+    def run(n, p, dt, ticks, one_by_one):
+        pos, vel, m = ics.plummer(n, seed=n)
+        ctx.upload(pos, vel, m)
+        if one_by_one:
+            for _ in range(ticks):
+                ctx.verlet_steps(p, dt, 1)
+        else:
+            ctx.verlet_steps(p, dt, ticks)
+        return ctx.download()
+    p = make_params(1.0, 0.01, method=DIRECT, precision=prec)
+    q = make_params(1.0, 0.02, method=DIRECT, precision=prec)
+    for n, pp, dt in ((1000, p, 1e-3), (1000, p, 2e-3), (1000, q, 2e-3), (3000, q, 2e-3),
+                      (1000, p, 1e-3)):
+        a = run(n, pp, dt, 7, False)
+        b = run(n, pp, dt, 7, True)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y), (n, dt)
