@@ -176,7 +176,7 @@ enum WsSlot {
   WS_ENTRIES, WS_ENTRIES_ALT, WS_EOFF, WS_ENTRY_BODY,
   WS_DIRECT_PART, WS_ADJ0, WS_ADJ1, WS_ADJ2, WS_ADJ3, WS_ADJ4,
   WS_ENS0, WS_ENS1, WS_ENS2, WS_ENS3, WS_ENS4, WS_ENS5, WS_ENS6, WS_ENS7,
-  WS_GROUPS, WS_GROUP_OFF, WS_GROUP_CTR, WS_GROUP_POOL, WS_GROUP_ITEMS, WS_SHARE_PERM,
+  WS_GROUPS, WS_GROUP_OFF, WS_GROUP_CTR, WS_GROUP_POOL, WS_GROUP_ITEMS, WS_SHARE_PERM, WS_BODY_IN,
   WS_COUNT_
 };
 static_assert(WS_COUNT_ <= sizeof(phys_ctx::ws) / sizeof(DevBuf), "workspace slots");

@@ -137,11 +137,15 @@ __global__ void bbox_final_kernel(int nparts, const double* __restrict__ part, d
 // ---------------------------------------------------------------------------
 // K3: descent keys.  hi = octants 0..20 (octant d in bits 62-3d..60-3d), lo =
 // octants 21..39 (bits 56..0); octants below D* are zero for every body.
+// Each body's (x, y, z, m) also goes into one 32-byte record, so that the
+// gather into key order after the sort reads one sector per body instead of
+// one per component.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock)
 keys_kernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
-            const double* __restrict__ z, const TreeHeader* __restrict__ hdr,
-            uint64_t* __restrict__ khi, uint64_t* __restrict__ klo, uint32_t* __restrict__ idx) {
+            const double* __restrict__ z, const double* __restrict__ m,
+            const TreeHeader* __restrict__ hdr, uint64_t* __restrict__ khi,
+            uint64_t* __restrict__ klo, uint32_t* __restrict__ idx, double4* __restrict__ rec) {
   const double c0 = hdr->center[0], c1 = hdr->center[1], c2 = hdr->center[2];
   const double h0 = hdr->half;
   const int D = hdr->dstar;
@@ -165,6 +169,7 @@ keys_kernel(int64_t n, const double* __restrict__ x, const double* __restrict__ 
     khi[i] = kh;
     klo[i] = kl;
     idx[i] = (uint32_t)i;
+    rec[i] = make_double4(px, py, pz, m[i]);
   }
 }
 
@@ -222,9 +227,8 @@ __global__ void run_fixup_kernel(int64_t n, const uint64_t* __restrict__ hs,
 
 __global__ void __launch_bounds__(kBlock)
 gather_sorted_kernel(int64_t n, const uint32_t* __restrict__ perm, const uint64_t* __restrict__ klo,
-                     const double* __restrict__ x, const double* __restrict__ y,
-                     const double* __restrict__ z, const double* __restrict__ m,
-                     uint64_t* __restrict__ lo_s, double4* __restrict__ body64,
+                     const double4* __restrict__ rec, uint64_t* __restrict__ lo_s,
+                     double4* __restrict__ body64,
                      float4* __restrict__ body_hi, float4* __restrict__ body_lo,
                      Body32x2* __restrict__ body2, const int32_t* status) {
   if (sort_failed(status)) return;
@@ -232,7 +236,7 @@ gather_sorted_kernel(int64_t n, const uint32_t* __restrict__ perm, const uint64_
        p += (int64_t)gridDim.x * blockDim.x) {
     const uint32_t i = perm[p];
     lo_s[p] = klo[i];
-    const double4 b = make_double4(x[i], y[i], z[i], m[i]);
+    const double4 b = rec[i];
     body64[p] = b;
     if (body_hi) {
       float4 h, l;
@@ -950,7 +954,10 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
   PHYS_LAUNCH(c, bbox_final_kernel, 1, 32, 0, kBboxGrid, c->d_partials, p->theta, c->d_hdr,
               c->d_status);
   PHYS_CUDA(c, cudaEventRecord(c->ev[3], c->stream));
-  PHYS_LAUNCH(c, keys_kernel, grid_for(n), kBlock, 0, n, c->x, c->y, c->z, c->d_hdr, khi, klo, idx);
+  double4* rec = nullptr;
+  PHYS_TRY(ws_alloc(c, WS_BODY_IN, n, &rec));
+  PHYS_LAUNCH(c, keys_kernel, grid_for(n), kBlock, 0, n, c->x, c->y, c->z, c->m, c->d_hdr, khi,
+              klo, idx, rec);
   PHYS_CUDA(c, cudaEventRecord(c->ev[4], c->stream));
   bool in_alt = false;
   PHYS_TRY(radix_sort_u64(c, khi, idx, khi_alt, idx_alt, n, 0, 64, &in_alt));
@@ -958,8 +965,8 @@ int bh_build(phys_ctx* c, const phys_params* p, bool need_f32, BhTree* t, bool n
   uint32_t* perm = in_alt ? idx_alt : idx;
   uint32_t* spare = in_alt ? idx : idx_alt;
   PHYS_LAUNCH(c, run_fixup_kernel, grid_for(n), kBlock, 0, n, hs, perm, klo, spare, c->d_status);
-  PHYS_LAUNCH(c, gather_sorted_kernel, grid_for(n), kBlock, 0, n, perm, klo, c->x, c->y, c->z,
-              c->m, lo_s, body64, body_hi, body_lo, body2, c->d_status);
+  PHYS_LAUNCH(c, gather_sorted_kernel, grid_for(n), kBlock, 0, n, perm, klo, rec, lo_s, body64,
+              body_hi, body_lo, body2, c->d_status);
   PHYS_CUDA(c, cudaEventRecord(c->ev[5], c->stream));
   PHYS_LAUNCH(c, lcp_count_kernel, grid_for(n + 1), kBlock, 0, n, hs, lo_s, c->d_hdr, L, cnt);
   // bucket leaves: count only the cells that survive (no full tree)
