@@ -159,23 +159,17 @@ vjp_kernel(int64_t n, int64_t slice_len, const double* __restrict__ x,
   p[3 * n + j] = gm;
 }
 
-// xbar += G sum_slices u ; mbar += G sum_slices gm (slice order fixed)
+// xbar += G sum_slices u ; mbar += G sum_slices gm (slice order fixed): one
+// thread per (target, component), its slices' loads in flight together.
 __global__ void vjp_reduce(int64_t n, int nsl, const double* __restrict__ part, double G,
                            double* __restrict__ xbar, double* __restrict__ mbar) {
-  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
-       j += (int64_t)gridDim.x * blockDim.x) {
-    double u0 = 0, u1 = 0, u2 = 0, g = 0;
-    for (int s = 0; s < nsl; ++s) {
-      const double* p = part + (size_t)s * 4 * n;
-      u0 += p[j];
-      u1 += p[n + j];
-      u2 += p[2 * n + j];
-      g += p[3 * n + j];
-    }
-    xbar[j] += G * u0;
-    xbar[n + j] += G * u1;
-    xbar[2 * n + j] += G * u2;
-    mbar[j] += G * g;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < 4 * n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(e / n);
+    const int64_t j = e - k * n;
+    const double u = slice_sum(part + k * n + j, 4 * (size_t)n, nsl);
+    double* out = k < 3 ? xbar + k * n + j : mbar + j;
+    *out += G * u;
   }
 }
 
@@ -220,7 +214,8 @@ int vjp(phys_ctx* c, const phys_params* p, Adj& a, const double* x) {
   dim3 grid((unsigned)ceil_div(n, kTile), (unsigned)nsl);
   PHYS_LAUNCH(c, vjp_kernel, grid, kTile, 0, n, slice_len, x, x + n, x + 2 * n, c->m, a.abar,
               a.abar + n, a.abar + 2 * n, p->eps * p->eps, a.vpart);
-  PHYS_LAUNCH(c, vjp_reduce, grid_for(n), kBlock, 0, n, (int)nsl, a.vpart, p->G, a.xbar, a.mbar);
+  PHYS_LAUNCH(c, vjp_reduce, grid_for(4 * n), kBlock, 0, n, (int)nsl, a.vpart, p->G, a.xbar,
+              a.mbar);
   return PHYS_OK;
 }
 

@@ -303,6 +303,23 @@ __device__ __forceinline__ float rsqrt_sfu(float x) {
   return y;
 }
 
+// sum_{s < nsl} p[s stride], added in slice order from 0.0 (the order the
+// results depend on); the loads go out eight slices at a time.
+__device__ __forceinline__ double slice_sum(const double* __restrict__ p, size_t stride,
+                                            int nsl) {
+  double a = 0.0;
+  int s = 0;
+  for (; s + 8 <= nsl; s += 8) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = p[(size_t)(s + u) * stride];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) a += v[u];
+  }
+  for (; s < nsl; ++s) a += p[(size_t)s * stride];
+  return a;
+}
+
 // True when a radix sort earlier in this call gave up a bounded wait
 // (kStatTimeout in the status word): its output need not be a permutation.
 // Kernels that index with a sort's output, or read records built from one,

@@ -312,27 +312,25 @@ direct_f32c_kernel(int64_t n, int64_t t0, int64_t t1, int64_t slice_len,
 }
 
 // Sum slice partials in slice order and apply G (and m_i for forces), for
-// targets [t0, t1) of partials laid out with stride n per component.
+// targets [t0, t1) of partials laid out with stride n per component: one
+// thread per (target, component), its slices' loads in flight together.
 __global__ void slice_reduce_kernel(int64_t n, int64_t t0, int64_t t1, int nslices,
                                     const double* __restrict__ part,
                                     const double* __restrict__ m, double G, int want_force,
                                     double* __restrict__ ox, double* __restrict__ oy,
                                     double* __restrict__ oz, int32_t* status) {
-  for (int64_t i = t0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < t1;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    double ax = 0.0, ay = 0.0, az = 0.0;
-    for (int s = 0; s < nslices; ++s) {
-      const double* p = part + (size_t)s * 3 * n;
-      ax += p[i];
-      ay += p[n + i];
-      az += p[2 * n + i];
-    }
-    double sc = want_force ? G * m[i] : G;
-    ox[i] = ax * sc;
-    oy[i] = ay * sc;
-    oz[i] = az * sc;
-    if (!isfinite(ax) || !isfinite(ay) || !isfinite(az)) atomicOr(status, kStatNonfinite);
+  const int64_t nt = t1 - t0;
+  bool bad = false;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < 3 * nt;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(e / nt);
+    const int64_t i = t0 + (e - k * nt);
+    const double a = slice_sum(part + k * n + i, 3 * (size_t)n, nslices);
+    const double sc = want_force ? G * m[i] : G;
+    (k == 0 ? ox : k == 1 ? oy : oz)[i] = a * sc;
+    bad |= !isfinite(a);
   }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(status, kStatNonfinite);
 }
 
 // Subset of targets (index list), all sources; one thread per (target,
@@ -461,7 +459,7 @@ int direct_eval(phys_ctx* c, const phys_params* p, bool want_force, double* ox, 
                   p->G, (float)eps2, (int)want_force, ox, oy, oz, part, c->d_status);
     }
     if (nsl > 1) {
-      int g = (int)min64(ceil_div(nt, 256), 148 * 8);
+      int g = (int)min64(ceil_div(3 * nt, 256), 148 * 8);
       PHYS_LAUNCH(c, slice_reduce_kernel, g, 256, 0, n, t0, t1, (int)nsl, part, c->m, p->G,
                   (int)want_force, ox, oy, oz, c->d_status);
     }
@@ -498,7 +496,8 @@ cudaError_t direct_accel_launch_scratch(cudaStream_t s, int64_t n, const double*
                                               ox, oy, oz, part, status);
   }
   if (nsl > 1)
-    slice_reduce_kernel<<<g, 256, 0, s>>>(n, 0, n, (int)nsl, part, m, G, 0, ox, oy, oz, status);
+    slice_reduce_kernel<<<(int)min64(ceil_div(3 * n, 256), 148 * 8), 256, 0, s>>>(
+        n, 0, n, (int)nsl, part, m, G, 0, ox, oy, oz, status);
   return cudaGetLastError();  // the launch error, if any (and clears it)
 }
 
@@ -522,7 +521,7 @@ int direct_targets(phys_ctx* c, const phys_params* p, int64_t nt, const int64_t*
   PHYS_LAUNCH(c, direct_targets_kernel, grid, kTile, 0, n, nt, d_tidx, slice_len, c->x, c->y,
               c->z, c->m, p->G, eps2, (int)exact, part, ox, oy, oz, c->d_status);
   if (!exact) {
-    int g = (int)min64(ceil_div(nt, 256), 148 * 8);
+    int g = (int)min64(ceil_div(3 * nt, 256), 148 * 8);
     PHYS_LAUNCH(c, slice_reduce_kernel, g, 256, 0, nt, 0, nt, (int)nsl, part, c->m, p->G, 0, ox,
                 oy, oz, c->d_status);
   }
