@@ -394,6 +394,15 @@ int phys_direct_accel_noalloc(int64_t n, const double* x, const double* y, const
  * bodies). */
 int phys_debug_set_wait_limit(phys_ctx* ctx, int64_t spins);
 
+/* No counterpart in the reference.  q[i] = a[i] / b[i] (host arrays of n)
+ * through the division of the tree's centre-of-mass recurrence
+ * (gravity_tree.rs:113-118 divides by the new total mass): a correction
+ * from the correctly rounded reciprocal of b where |a| and b lie in
+ * [2^-500, 2^501) (and b > 0), the IEEE division elsewhere.  Both are
+ * meant to give the correctly rounded quotient; tests compare q bit for
+ * bit with IEEE division. */
+int phys_debug_divide(phys_ctx* ctx, int64_t n, const double* a, const double* b, double* q);
+
 /* ---- measured pipe peaks (roofline denominators) ----------------------- */
 /* Times FFMA, packed FFMA2 (f32x2) and DFMA loops on every SM; returns
  * TFLOP/s counting an FMA as 2 flops (FFMA2 as 4). */

@@ -245,6 +245,7 @@ int adjoint(phys_ctx* c, const phys_params* p, double dt, int64_t nsteps, int64_
 // diag.cu
 int diagnostics(phys_ctx* c, double G, double* out5);
 int probe_peaks(phys_ctx* c, double* fp32, double* fp32x2, double* fp64);
+int debug_divide(phys_ctx* c, int64_t n, const double* a, const double* b, double* q);
 }  // namespace phys
 
 #define PHYS_LAUNCH_ON(c, strm, kernel, grid, block, smem, ...)            \
@@ -283,6 +284,36 @@ __device__ __forceinline__ double xsqrt(double a) { return __dsqrt_rn(a); }
 // glam DVec3::length_squared: (x*x + y*y) + z*z
 __device__ __forceinline__ double xlen2(double x, double y, double z) {
   return xadd(xadd(xmul(x, x), xmul(y, y)), xmul(z, z));
+}
+
+// a / b rounded to nearest from y = RN(1/b), computed ahead of a (Markstein's
+// correction: P. Markstein, "Computation of elementary functions on the IBM
+// RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990).  q0 = RN(a y)
+// lies within 1.5 ulp of a/b; q1 = RN(q0 + y RN(a - b q0)) within one ulp;
+// the remainder r1 = a - b q1 is then exact in an FMA, and RN(q1 + r1 y)
+// is RN(a/b): with b's significand B < 2^53 the term r1 (b y - 1) stays
+// below b |a/b - m| for every midpoint m (B^2 + B < 2^106), and a/b is never
+// a midpoint.  Valid while no step underflows or overflows, which
+// div_recip_num_ok(a) and div_recip_den_ok(b) guarantee (|a| and b in
+// [2^-500, 2^501); a = +0 also gives +0; only positive b is accepted; both
+// tests read the exponent bits on the integer pipe).  A chain of these
+// divisions has five dependent operations per step, where a full division
+// recomputes the reciprocal on the critical path.
+__device__ __forceinline__ double div_recip(double a, double b, double y) {
+  const double q0 = __dmul_rn(a, y);
+  const double r0 = __fma_rn(-b, q0, a);
+  const double q1 = __fma_rn(r0, y, q0);
+  const double r1 = __fma_rn(-b, q1, a);
+  return __fma_rn(r1, y, q1);
+}
+__device__ __forceinline__ bool div_recip_den_ok(double b) {
+  // sign clear and biased exponent in [523, 1523] (a negative b shifts to a
+  // negative value, far out of range as unsigned)
+  return (unsigned long long)(__double_as_longlong(b) >> 52) - 523ull <= 1000ull;
+}
+__device__ __forceinline__ bool div_recip_num_ok(double a) {
+  const long long bits = __double_as_longlong(a);
+  return (unsigned long long)((bits >> 52) & 0x7ff) - 523ull <= 1000ull || bits == 0;
 }
 
 // Knuth two-sum: s + e == a + b exactly.

@@ -1098,6 +1098,12 @@ int phys_debug_set_wait_limit(phys_ctx* c, int64_t spins) {
   return PHYS_OK;
 }
 
+int phys_debug_divide(phys_ctx* c, int64_t n, const double* a, const double* b, double* q) {
+  if (!c || n < 0 || (n > 0 && (!a || !b || !q))) return PHYS_ERR_ARG;
+  PHYS_ENTER(c);
+  return debug_divide(c, n, a, b, q);
+}
+
 int phys_probe_peaks(phys_ctx* c, double* fp32, double* fp32x2, double* fp64) {
   if (!c || !fp32 || !fp32x2 || !fp64) return PHYS_ERR_ARG;
   PHYS_ENTER(c);

@@ -604,11 +604,66 @@ gather_entries_kernel(int64_t total, const uint64_t* __restrict__ entries,
 // (com_recurrence_long_kernel), the rest on a thread each.
 constexpr int kLongChain = 2048;
 
-// One thread per cell runs the recurrence over the cell's gathered bodies;
-// the next batch's loads are issued before the current batch's chain of
-// dependent divides, so the chain (the critical path: a multiply, an add
-// and a divide per body) does not wait for memory.  Cells of kLongChain
-// bodies or more are appended to `longs` (count in longs[nnodes]) instead.
+// The reference recurrence over a cell's gathered bodies eb[e0, e1)
+// (gravity_tree.rs:113-118): M' = M + m, and when M' > 0,
+// c = (c M + x m) / M' per coordinate.  kFast divides through div_recip by
+// RN(1/M'), which depends only on the mass chain and so is computed off the
+// critical path (a multiply, an add and the five operations of div_recip per
+// body instead of a multiply, an add and a division); it returns false when
+// a step left div_recip's range (or M' <= 0), and the caller then reruns the
+// cell with kFast = false, the reference's division.  Both give the IEEE
+// result of every step.  The next batch's loads are issued before the
+// current batch's chain, so the chain does not wait for memory.
+template <bool kFast>
+__device__ __forceinline__ bool com_chain(const double4* __restrict__ eb, int64_t e0, int64_t e1,
+                                          double4& out) {
+  double M = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
+  bool ok = true;
+  auto step = [&](const double4 b) {
+    const double nt = xadd(M, b.w);
+    if (kFast) {
+      const double y = __drcp_rn(nt);
+      const double ax = xadd(xmul(cx, M), xmul(b.x, b.w));
+      const double ay = xadd(xmul(cy, M), xmul(b.y, b.w));
+      const double az = xadd(xmul(cz, M), xmul(b.z, b.w));
+      ok &= div_recip_den_ok(nt) & div_recip_num_ok(ax) & div_recip_num_ok(ay) &
+            div_recip_num_ok(az);
+      cx = div_recip(ax, nt, y);
+      cy = div_recip(ay, nt, y);
+      cz = div_recip(az, nt, y);
+    } else if (nt > 0.0) {
+      cx = xdiv(xadd(xmul(cx, M), xmul(b.x, b.w)), nt);
+      cy = xdiv(xadd(xmul(cy, M), xmul(b.y, b.w)), nt);
+      cz = xdiv(xadd(xmul(cz, M), xmul(b.z, b.w)), nt);
+    }
+    M = nt;
+  };
+  constexpr int kB = 8;
+  double4 cur[kB], nxt[kB];
+#pragma unroll
+  for (int u = 0; u < kB; ++u)
+    cur[u] = e0 + u < e1 ? eb[e0 + u] : make_double4(0.0, 0.0, 0.0, 0.0);
+  for (int64_t e = e0; e < e1; e += kB) {
+#pragma unroll
+    for (int u = 0; u < kB; ++u)
+      nxt[u] = e + kB + u < e1 ? eb[e + kB + u] : make_double4(0.0, 0.0, 0.0, 0.0);
+    if (e + kB <= e1) {
+#pragma unroll
+      for (int u = 0; u < kB; ++u) step(cur[u]);
+    } else {
+      for (int u = 0; u < kB; ++u)
+        if (e + u < e1) step(cur[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < kB; ++u) cur[u] = nxt[u];
+  }
+  out = make_double4(cx, cy, cz, M);
+  return ok;
+}
+
+// One thread per cell runs com_chain over the cell's gathered bodies.
+// Cells of kLongChain bodies or more are appended to `longs` (count in
+// longs[nnodes]) instead.
 __global__ void __launch_bounds__(kBlock)
 com_recurrence_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
                       const double4* __restrict__ eb, double4* __restrict__ mc,
@@ -631,33 +686,9 @@ com_recurrence_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
       longs[atomicAdd(&longs[nnodes], 1)] = (int32_t)k;
       continue;
     }
-    double M = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
-    constexpr int kB = 8;
-    double4 cur[kB], nxt[kB];
-#pragma unroll
-    for (int u = 0; u < kB; ++u)
-      cur[u] = e0 + u < e1 ? eb[e0 + u] : make_double4(0.0, 0.0, 0.0, 0.0);
-    for (int64_t e = e0; e < e1; e += kB) {
-#pragma unroll
-      for (int u = 0; u < kB; ++u)
-        nxt[u] = e + kB + u < e1 ? eb[e + kB + u] : make_double4(0.0, 0.0, 0.0, 0.0);
-#pragma unroll
-      for (int u = 0; u < kB; ++u) {
-        if (e + u < e1) {
-          const double4 b = cur[u];
-          const double nt = xadd(M, b.w);
-          if (nt > 0.0) {
-            cx = xdiv(xadd(xmul(cx, M), xmul(b.x, b.w)), nt);
-            cy = xdiv(xadd(xmul(cy, M), xmul(b.y, b.w)), nt);
-            cz = xdiv(xadd(xmul(cz, M), xmul(b.z, b.w)), nt);
-          }
-          M = nt;
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < kB; ++u) cur[u] = nxt[u];
-    }
-    mc[k] = make_double4(cx, cy, cz, M);
+    double4 r;
+    if (!com_chain<true>(eb, e0, e1, r)) com_chain<false>(eb, e0, e1, r);
+    mc[k] = r;
   }
 }
 
@@ -666,7 +697,49 @@ com_recurrence_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
 // while lanes 0, 1 and 2 run the x, y and z chains of the current 32 from
 // shared memory, each also running the mass sum (the same additions in the
 // same order, so the three agree).  Memory latency hides behind the chains.
+// kFast as in com_chain; the return value is the warp's.
 constexpr int kLongWarps = 4;
+template <bool kFast>
+__device__ __forceinline__ bool com_chain_warp(const double4* __restrict__ eb, int64_t e0,
+                                               int64_t e1, double4* buf, int lane,
+                                               double4& out) {
+  const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
+  double M = 0.0, cc = 0.0;  // lane j < 3: coordinate j
+  bool ok = true;
+  auto step = [&](double p, double mm) {
+    const double nt = xadd(M, mm);
+    if (kFast) {
+      const double y = __drcp_rn(nt);
+      const double a = xadd(xmul(cc, M), xmul(p, mm));
+      ok &= div_recip_den_ok(nt) & div_recip_num_ok(a);
+      cc = div_recip(a, nt, y);
+    } else if (nt > 0.0) {
+      cc = xdiv(xadd(xmul(cc, M), xmul(p, mm)), nt);
+    }
+    M = nt;
+  };
+  double4 v = e0 + lane < e1 ? eb[e0 + lane] : zero;
+  for (int64_t e = e0; e < e1; e += 32) {
+    buf[lane] = v;
+    __syncwarp();
+    v = e + 32 + lane < e1 ? eb[e + 32 + lane] : zero;
+    const int cnt = (int)min((int64_t)32, e1 - e);
+    if (lane < 3) {
+      const double* q = reinterpret_cast<const double*>(buf);
+      if (cnt == 32) {
+#pragma unroll 8
+        for (int u = 0; u < 32; ++u) step(q[4 * u + lane], q[4 * u + 3]);
+      } else {
+        for (int u = 0; u < cnt; ++u) step(q[4 * u + lane], q[4 * u + 3]);
+      }
+    }
+    __syncwarp();
+  }
+  const double cy = __shfl_sync(0xffffffffu, cc, 1), cz = __shfl_sync(0xffffffffu, cc, 2);
+  out = make_double4(cc, cy, cz, M);
+  return !__any_sync(0xffffffffu, !ok);
+}
+
 __global__ void __launch_bounds__(32 * kLongWarps)
 com_recurrence_long_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
                            const double4* __restrict__ eb, double4* __restrict__ mc,
@@ -678,28 +751,24 @@ com_recurrence_long_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
   for (int i = blockIdx.x * kLongWarps + w; i < nlong; i += gridDim.x * kLongWarps) {
     const int k = longs[i];
     const int64_t e0 = eoff[k], e1 = eoff[k + 1];
-    const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
-    double M = 0.0, cc = 0.0;  // lane j < 3: coordinate j
-    double4 v = e0 + lane < e1 ? eb[e0 + lane] : zero;
-    for (int64_t e = e0; e < e1; e += 32) {
-      buf[w][lane] = v;
-      __syncwarp();
-      v = e + 32 + lane < e1 ? eb[e + 32 + lane] : zero;
-      const int cnt = (int)min((int64_t)32, e1 - e);
-      if (lane < 3) {
-        const double* q = reinterpret_cast<const double*>(&buf[w][0]);
-#pragma unroll 8
-        for (int u = 0; u < cnt; ++u) {
-          const double p = q[4 * u + lane], mm = q[4 * u + 3];
-          const double nt = xadd(M, mm);
-          if (nt > 0.0) cc = xdiv(xadd(xmul(cc, M), xmul(p, mm)), nt);
-          M = nt;
-        }
-      }
-      __syncwarp();
-    }
-    const double cy = __shfl_sync(0xffffffffu, cc, 1), cz = __shfl_sync(0xffffffffu, cc, 2);
-    if (lane == 0) mc[k] = make_double4(cc, cy, cz, M);
+    double4 r;
+    if (!com_chain_warp<true>(eb, e0, e1, buf[w], lane, r))
+      com_chain_warp<false>(eb, e0, e1, buf[w], lane, r);
+    if (lane == 0) mc[k] = r;
+  }
+}
+
+// q[i] = a[i] / b[i] through the centre-of-mass chains' division: div_recip
+// where its range holds, the IEEE division elsewhere (a test-only check
+// that both give the correctly rounded quotient).
+__global__ void __launch_bounds__(kBlock)
+debug_divide_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                    double* __restrict__ q) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double x = a[i], d = b[i];
+    q[i] = div_recip_den_ok(d) && div_recip_num_ok(x) ? div_recip(x, d, __drcp_rn(d))
+                                                      : xdiv(x, d);
   }
 }
 
@@ -1209,6 +1278,20 @@ int bh_export(phys_ctx* c, const phys_params* p, int64_t cap, int64_t* nnodes, i
     if (leaf && body_leaf)
       for (int q = lk.y; q < lk.z; ++q) body_leaf[perm[q]] = k;
   }
+  return PHYS_OK;
+}
+
+int debug_divide(phys_ctx* c, int64_t n, const double* a, const double* b, double* q) {
+  if (n <= 0) return PHYS_OK;
+  int st = PHYS_OK;
+  double* d = (double*)ws_get(c, WS_ADJ2, sizeof(double) * 3 * n, &st);
+  if (st) return st;
+  const size_t bytes = sizeof(double) * (size_t)n;
+  PHYS_CUDA(c, cudaMemcpyAsync(d, a, bytes, cudaMemcpyHostToDevice, c->stream));
+  PHYS_CUDA(c, cudaMemcpyAsync(d + n, b, bytes, cudaMemcpyHostToDevice, c->stream));
+  PHYS_LAUNCH(c, debug_divide_kernel, grid_for(n), kBlock, 0, n, d, d + n, d + 2 * n);
+  PHYS_CUDA(c, cudaMemcpyAsync(q, d + 2 * n, bytes, cudaMemcpyDeviceToHost, c->stream));
+  PHYS_CUDA(c, cudaStreamSynchronize(c->stream));
   return PHYS_OK;
 }
 

@@ -56,6 +56,7 @@ EXPORTED = [
     "phys_nfw_forces", "phys_set_nfw_halo", "phys_state_upload_sector_state",
     "phys_state_download_sector_state", "phys_debug_set_wait_limit", "phys_share_chunk",
     "phys_gravity_accel_share", "phys_gravity_accel_unshare", "phys_verlet_tick_host",
+    "phys_debug_divide",
 ]
 
 
@@ -153,6 +154,7 @@ def load_library(path=None):
         "phys_state_download_sector_state": ([_VP, _I64, _I64, _I64, _D, _D, _D],
                                              ctypes.c_int),
         "phys_debug_set_wait_limit": ([_VP, i64], ctypes.c_int),
+        "phys_debug_divide": ([_VP, i64, _D, _D, _D], ctypes.c_int),
         "phys_share_chunk": ([i64, i32], i64),
         "phys_gravity_accel_share": ([_VP, P, i32, i32, _VP], ctypes.c_int),
         "phys_gravity_accel_unshare": ([_VP, i32, _VP], ctypes.c_int),
@@ -231,6 +233,17 @@ class Context:
         a negative value restores the default."""
         self._check(self.lib.phys_debug_set_wait_limit(self.h, int(spins)),
                     "phys_debug_set_wait_limit")
+
+    def debug_divide(self, a, b):
+        """a / b through the tree's centre-of-mass division (tests only)."""
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        if a.shape != b.shape or a.ndim != 1:
+            raise ValueError("a and b must be 1-D arrays of one length")
+        q = np.empty_like(a)
+        self._check(self.lib.phys_debug_divide(self.h, a.shape[0], _p(a), _p(b), _p(q)),
+                    "phys_debug_divide")
+        return q
 
     # ---- state ----
     def upload(self, pos, vel, m):

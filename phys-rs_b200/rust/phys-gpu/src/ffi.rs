@@ -197,6 +197,8 @@ extern "C" {
 
     // ---- failure injection for tests ----
     pub fn phys_debug_set_wait_limit(ctx: *mut phys_ctx, spins: i64) -> c_int;
+    pub fn phys_debug_divide(ctx: *mut phys_ctx, n: i64, a: *const f64, b: *const f64,
+                             q: *mut f64) -> c_int;
 
     // ---- measured pipe peaks ----
     pub fn phys_probe_peaks(ctx: *mut phys_ctx, fp32_tflops: *mut f64, fp32x2_tflops: *mut f64,
