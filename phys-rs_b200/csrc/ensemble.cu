@@ -207,11 +207,14 @@ __device__ __forceinline__ int next_pow2(int v) {
 // for the same b are added by shuffles at the end.  Each round covers r
 // source quads: all r against a (two interleaved chains), one (the
 // stream's own) against b.
-template <bool kSkip, class S_t>
+// kR = 1 (49..64 bodies: one stream, b = 32 + l) fixes the layout at
+// compile time, so b's quad is a's and is loaded once; kR = 0 derives the
+// streams from N.
+template <bool kSkip, int kR, class S_t>
 __device__ void group_forces_f32c_split(S_t* S, int N, int gl, double Gc, float eps2f) {
   const float2 e2 = make_float2(eps2f, eps2f);
   const int nb = N - 32;
-  const int lps = next_pow2(nb), r = 32 / lps;
+  const int lps = kR ? 32 / kR : next_pow2(nb), r = kR ? kR : 32 / lps;
   const int st = gl / lps, tb = 32 + gl % lps;
   const int ta = gl;
   const int tbv = tb < N ? tb : ta;  // lanes without a valid b compute a dummy (discarded)
@@ -294,7 +297,10 @@ template <int G, int kMaxTC, bool kSkip, class S_t>
 __device__ __forceinline__ void group_forces_f32c_any(S_t* S, int N, int gl, double Gc,
                                                       float eps2f) {
   if (G == 32 && N > 32) {
-    group_forces_f32c_split<kSkip>(S, N, gl, Gc, eps2f);
+    if (N > 48)
+      group_forces_f32c_split<kSkip, 1>(S, N, gl, Gc, eps2f);
+    else
+      group_forces_f32c_split<kSkip, 0>(S, N, gl, Gc, eps2f);
     return;
   }
   if (kMaxTC == 1 || N <= G)
