@@ -175,6 +175,32 @@ def test_exact_forces_coincident(ctx):
     assert np.array_equal(f, oracle.bh_forces(pos, m, 1.0, 0.01, 0.5))
 
 
+@pytest.mark.parametrize("kind", ["tiny", "mixed"])
+def test_exact_com_outside_reciprocal_range(ctx, kind):
+    """The centre-of-mass chains divide through a reciprocal while the running
+    mass and the numerators lie in [2^-500, 2^501); a cell that leaves that
+    range is rerun with the IEEE division.  Masses near 1e-160 send every
+    chain there ("tiny"), every other body's ("mixed") only the cells whose
+    first inserted body is one of them.  20 000 bodies: cells of more than
+    2048 bodies take the warp form, the rest the thread form.  Tree and
+    forces stay bit-identical to the oracle (G = 1e300 keeps the tiny
+    masses' pair terms normal)."""
+    pos, _, m = ics.plummer(20000, seed=21)
+    m = m.copy()
+    if kind == "tiny":
+        m *= 1e-160
+        G = 1e300
+    else:
+        m[::2] *= 1e-160
+        G = 1.0
+    g = structure_check(ctx, pos, m)
+    assert (g["count"] >= 2048).any()
+    f = ctx.gravity_forces(bh(0.5, F64_EXACT, G=G))
+    ref = oracle.bh_forces(pos, m, G, 0.01, 0.5)
+    assert np.isfinite(ref).all() and (ref != 0).any()
+    assert np.array_equal(f, ref)
+
+
 @pytest.mark.parametrize("n", [4096, 65536])
 def test_f64_close_to_reference(ctx, n):
     pos, _, m = ics.plummer(n, seed=n)
