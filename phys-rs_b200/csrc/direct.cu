@@ -21,15 +21,24 @@ namespace {
 // loaded ahead), while lane t of warp 0 adds round k-1's terms of target t
 // in j order, skipping j == i as the reference does.  The divides and square
 // roots, whose latency bounded the one-thread-per-target form, run in
-// parallel; the sum is the reference's bit for bit.  What is left is the
-// ordered chain of N dependent f64 additions per component, the bound of
-// any exact form (1024 bodies: about 20 us per evaluation).
+// parallel; the sum is the reference's bit for bit.  The floor of any exact
+// form is the ordered chain of N - 1 dependent f64 additions per component
+// (an f64 add waits ≈ 8 cycles for the one before it: ≈ 4 us at N = 1024);
+// the kernel takes ≈ 4 times that.
 // ---------------------------------------------------------------------------
 constexpr int kXT = 8;                    // targets per block
 constexpr int kXJ = 64;                   // sources per round
 constexpr int kXCompute = kXT * kXJ / 2;  // compute threads: two targets each
-constexpr int kXBlock = 32 + kXCompute;   // warp 0 adds, the rest compute
+// Warp 0 adds; the compute warps are the first kXCompute / 32 warps whose
+// index is not a multiple of 4, so none shares warp 0's scheduler (warps are
+// spread over an SM's four schedulers by index): warps 1-3, 5-7, 9, 10 of
+// 12; warps 4, 8 and 11 return at once.  The round barrier is a named
+// barrier over the 9 working warps only.
+constexpr int kXWarps = 12;
+constexpr int kXBlock = 32 * kXWarps;
+constexpr int kXWorking = 32 + kXCompute;
 static_assert(kXT <= 32 && kXCompute % 32 == 0 && kXJ % 32 == 0, "exact block layout");
+static_assert(kXCompute / 32 == 8 && kXWorking == 288, "bar.sync count below");
 
 __global__ void __launch_bounds__(kXBlock)
 direct_exact_kernel(int64_t n, int64_t t0, int64_t t1, const double* __restrict__ x,
@@ -39,14 +48,18 @@ direct_exact_kernel(int64_t n, int64_t t0, int64_t t1, const double* __restrict_
                     int32_t* status) {
   __shared__ double term[2][3][kXT][kXJ + 1];  // [round parity][x, y, z][target][source]
   __shared__ double4 tgt[kXT];                 // x_i, y_i, z_i, G*m_i
-  const int tid = threadIdx.x;
+  const int w = threadIdx.x >> 5;
+  const int cw = (w % 4 == 0) ? -1 : w - 1 - w / 4;  // compute warp 0..7, or -1
+  if (w != 0 && (cw < 0 || cw >= kXCompute / 32)) return;  // idle: no barrier
+  // tid: warp 0 keeps its lanes; compute warp cw acts as threads 32 + 32 cw + lane
+  const int tid = w == 0 ? (int)threadIdx.x : 32 + cw * 32 + (int)(threadIdx.x & 31);
   const int64_t i0 = t0 + blockIdx.x * (int64_t)kXT;
   if (tid < kXT) {
     const int64_t i = i0 + tid;
     tgt[tid] = i < t1 ? make_double4(x[i], y[i], z[i], xmul(G, m[i]))
                       : make_double4(0.0, 0.0, 0.0, 0.0);
   }
-  __syncthreads();
+  asm volatile("bar.sync 1, 288;" ::: "memory");  // kXWorking
   const int64_t rounds = ceil_div(n, kXJ);
   // compute threads: source slot jj, targets ta and ta + kXT/2
   const int c = tid - 32, jj = c % kXJ, ta = c / kXJ;
@@ -105,7 +118,7 @@ direct_exact_kernel(int64_t n, int64_t t0, int64_t t1, const double* __restrict_
         fz = xadd(fz, tz[q]);
       }
     }
-    __syncthreads();
+    asm volatile("bar.sync 1, 288;" ::: "memory");  // kXWorking
   }
   if (tid >= 32) return;
   const int64_t i = i0 + tid;

@@ -693,46 +693,112 @@ com_recurrence_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
 }
 
 // The same recurrence for the cells listed by com_recurrence_kernel, a warp
-// per cell: the warp loads the next 32 bodies (one coalesced 1 KiB read)
-// while lanes 0, 1 and 2 run the x, y and z chains of the current 32 from
-// shared memory, each also running the mass sum (the same additions in the
-// same order, so the three agree).  Memory latency hides behind the chains.
-// kFast as in com_chain; the return value is the warp's.
+// per cell: the warp stages 32 bodies at a time in shared memory (one
+// coalesced 1 KiB read, the next batch's in flight) while lanes 0, 1 and 2
+// run the x, y and z chains.
 constexpr int kLongWarps = 4;
-template <bool kFast>
-__device__ __forceinline__ bool com_chain_warp(const double4* __restrict__ eb, int64_t e0,
-                                               int64_t e1, double4* buf, int lane,
-                                               double4& out) {
+struct LongStage {
+  double4 rec[2][32];           // two batches of body records (x, y, z, m)
+  double nt[2][32], y[2][32];   // per body: running mass M + m, RN(1/(M + m))
+};
+
+// The reference's form (com_chain<false> per coordinate lane): the fallback.
+__device__ void com_chain_warp_ieee(const double4* __restrict__ eb, int64_t e0, int64_t e1,
+                                   LongStage& S, int lane, double4& out) {
   const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
   double M = 0.0, cc = 0.0;  // lane j < 3: coordinate j
-  bool ok = true;
-  auto step = [&](double p, double mm) {
-    const double nt = xadd(M, mm);
-    if (kFast) {
-      const double y = __drcp_rn(nt);
-      const double a = xadd(xmul(cc, M), xmul(p, mm));
-      ok &= div_recip_den_ok(nt) & div_recip_num_ok(a);
-      cc = div_recip(a, nt, y);
-    } else if (nt > 0.0) {
-      cc = xdiv(xadd(xmul(cc, M), xmul(p, mm)), nt);
-    }
-    M = nt;
-  };
   double4 v = e0 + lane < e1 ? eb[e0 + lane] : zero;
   for (int64_t e = e0; e < e1; e += 32) {
-    buf[lane] = v;
+    S.rec[0][lane] = v;
     __syncwarp();
     v = e + 32 + lane < e1 ? eb[e + 32 + lane] : zero;
     const int cnt = (int)min((int64_t)32, e1 - e);
     if (lane < 3) {
-      const double* q = reinterpret_cast<const double*>(buf);
-      if (cnt == 32) {
-#pragma unroll 8
-        for (int u = 0; u < 32; ++u) step(q[4 * u + lane], q[4 * u + 3]);
-      } else {
-        for (int u = 0; u < cnt; ++u) step(q[4 * u + lane], q[4 * u + 3]);
+      const double* q = reinterpret_cast<const double*>(&S.rec[0][0]);
+      for (int u = 0; u < cnt; ++u) {
+        const double p = q[4 * u + lane], mm = q[4 * u + 3];
+        const double nt = xadd(M, mm);
+        if (nt > 0.0) cc = xdiv(xadd(xmul(cc, M), xmul(p, mm)), nt);
+        M = nt;
       }
     }
+    __syncwarp();
+  }
+  const double cy = __shfl_sync(0xffffffffu, cc, 1), cz = __shfl_sync(0xffffffffu, cc, 2);
+  out = make_double4(cc, cy, cz, M);
+}
+
+// The fast form: per body a multiply, an add and div_recip's five
+// operations, with nothing else on the chain.  The running masses of a
+// batch (the reference's additions, in order) are summed by lane 0 while the
+// batch before it runs, and the whole warp then forms the batch's 32
+// reciprocals at once (__drcp_rn, correctly rounded, as div_recip requires),
+// so the chain's loop over a full batch has no branch and its shared-memory
+// loads can be issued ahead.  Returns false (warp-uniform) when a step left
+// div_recip's range or the running mass was not positive; the caller then
+// reruns the cell in the reference's form.
+__device__ bool com_chain_warp_fast(const double4* __restrict__ eb, int64_t e0, int64_t e1,
+                                    LongStage& S, int lane, double4& out) {
+  const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
+  const int64_t len = e1 - e0;
+  S.rec[0][lane] = lane < len ? eb[e0 + lane] : zero;
+  double4 v = 32 + lane < len ? eb[e0 + 32 + lane] : zero;
+  __syncwarp();
+  if (lane == 0) {  // running masses of batch 0
+    double M = 0.0;
+    const int c0 = (int)min((int64_t)32, len);
+    for (int u = 0; u < c0; ++u) {
+      M = xadd(M, S.rec[0][u].w);
+      S.nt[0][u] = M;
+    }
+  }
+  __syncwarp();
+  S.y[0][lane] = __drcp_rn(S.nt[0][lane]);  // lanes past the batch: unused
+  __syncwarp();
+  bool ok = true;
+  double cc = 0.0, M = 0.0;  // lane j < 3: coordinate j; M = mass before the body
+  for (int64_t base = e0; base < e1; base += 32) {
+    const int cur = (int)(((base - e0) >> 5) & 1), nxt = cur ^ 1;
+    const int cnt = (int)min((int64_t)32, e1 - base);
+    const int cntn = (int)max((int64_t)0, min((int64_t)32, e1 - base - 32));
+    if (cntn > 0) S.rec[nxt][lane] = v;
+    __syncwarp();
+    v = base + 64 + lane < e1 ? eb[base + 64 + lane] : zero;
+    if (lane < 3) {
+      const double* __restrict__ rc = reinterpret_cast<const double*>(&S.rec[cur][0]);
+      const double* __restrict__ rn = reinterpret_cast<const double*>(&S.rec[nxt][0]);
+      const double* __restrict__ ntc = S.nt[cur];
+      const double* __restrict__ yc = S.y[cur];
+      auto step = [&](int u) {
+        const double nt = ntc[u];
+        const double a = xadd(xmul(cc, M), xmul(rc[4 * u + lane], rc[4 * u + 3]));
+        ok &= div_recip_den_ok(nt) & div_recip_num_ok(a);
+        cc = div_recip(a, nt, yc[u]);
+        M = nt;
+      };
+      if (cnt == 32) {
+        // the next batch's running masses, in registers until the batch is
+        // done (a store into the arrays the loop reads would keep the
+        // loads behind it)
+        double Mn[32];
+        double acc = ntc[31];  // running mass before the next batch
+#pragma unroll
+        for (int u = 0; u < 32; ++u) {
+          step(u);
+          acc = xadd(acc, rn[4 * u + 3]);  // bodies past cntn: never stored
+          Mn[u] = acc;
+        }
+        if (lane == 0) {
+#pragma unroll
+          for (int u = 0; u < 32; ++u)
+            if (u < cntn) S.nt[nxt][u] = Mn[u];
+        }
+      } else {  // the last batch of the cell
+        for (int u = 0; u < cnt; ++u) step(u);
+      }
+    }
+    __syncwarp();
+    if (cntn > 0) S.y[nxt][lane] = __drcp_rn(S.nt[nxt][lane]);
     __syncwarp();
   }
   const double cy = __shfl_sync(0xffffffffu, cc, 1), cz = __shfl_sync(0xffffffffu, cc, 2);
@@ -745,16 +811,17 @@ com_recurrence_long_kernel(int64_t nnodes, const int32_t* __restrict__ eoff,
                            const double4* __restrict__ eb, double4* __restrict__ mc,
                            const int32_t* __restrict__ longs, const int32_t* status) {
   if (sort_failed(status)) return;
-  __shared__ double4 buf[kLongWarps][32];
+  __shared__ LongStage stage[kLongWarps];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int nlong = min(longs[nnodes], (int32_t)nnodes);
   for (int i = blockIdx.x * kLongWarps + w; i < nlong; i += gridDim.x * kLongWarps) {
     const int k = longs[i];
     const int64_t e0 = eoff[k], e1 = eoff[k + 1];
     double4 r;
-    if (!com_chain_warp<true>(eb, e0, e1, buf[w], lane, r))
-      com_chain_warp<false>(eb, e0, e1, buf[w], lane, r);
+    if (!com_chain_warp_fast(eb, e0, e1, stage[w], lane, r))
+      com_chain_warp_ieee(eb, e0, e1, stage[w], lane, r);
     if (lane == 0) mc[k] = r;
+    __syncwarp();
   }
 }
 
